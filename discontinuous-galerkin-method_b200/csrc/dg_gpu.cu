@@ -1,0 +1,864 @@
+// dg_gpu.cu — host side of the sm_100a DG engine: the C ABI of include/dg_gpu.h.
+//
+// dg_gpu_init validates the reference's set-up arrays, renumbers elements along a Hilbert curve
+// of their centroids, converts the index maps into compact face codes and the per-element
+// operators into geometric factors (or keeps the reference's own operators for DG_FP64_REF),
+// and uploads everything.  dg_gpu_step replays a CUDA graph of `graph_steps` steps, each step
+// being one velocity and one stress launch (the stress launch also records the receivers).
+#include "dg_gpu.h"
+#include "dg_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using namespace dg;
+
+namespace {
+
+thread_local std::string g_last;
+
+int cuda_fail(cudaError_t e, const char* what, int line) {
+  char buf[512];
+  snprintf(buf, sizeof buf, "%s (line %d): %s", what, line, cudaGetErrorString(e));
+  g_last = buf;
+  return e == cudaErrorMemoryAllocation ? DG_ERR_NOMEM : DG_ERR_CUDA;
+}
+#define CK(x)                                                \
+  do {                                                       \
+    cudaError_t e_ = (x);                                    \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #x, __LINE__); \
+  } while (0)
+
+int fail(int code, const char* msg) {
+  g_last = msg;
+  return code;
+}
+
+// Hilbert index of (x, y) on a 2^16 grid (the classic rotate-and-accumulate walk).
+uint64_t hilbert(uint32_t x, uint32_t y) {
+  uint64_t d = 0;
+  for (uint32_t s = 1u << 15; s > 0; s >>= 1) {
+    uint32_t rx = (x & s) > 0, ry = (y & s) > 0;
+    d += (uint64_t)s * s * ((3 * rx) ^ ry);
+    if (ry == 0) {
+      if (rx == 1) { x = s - 1 - (x & (s - 1)) + (x & ~(s - 1)); y = s - 1 - (y & (s - 1)) + (y & ~(s - 1)); }
+      uint32_t t = x; x = y; y = t;
+    }
+  }
+  return d;
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+};
+
+}  // namespace
+
+struct MeshHostInfo {
+  long K = 0;
+  int Kp = 0, S = 0, n_rec = 0;
+  long steps = 0;
+  std::vector<int> new_of_old;  // caller element -> internal element
+  int* d_new_of_old = nullptr;
+  double dt = 0;
+  int elem_blocks = 0, rec_blocks = 0;
+  long sponge_elems = 0;
+};
+
+struct dg_gpu_ctx {
+  int device = 0;
+  int precision = DG_FP64;
+  bool is_double = true;
+  bool kahan = false;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  std::vector<MeshHostInfo> mi;
+  std::vector<MeshDev<double>> md_d;
+  std::vector<MeshDev<float>> md_f;
+  MeshDev<double>* d_tab_d = nullptr;
+  MeshDev<float>* d_tab_f = nullptr;
+  int2* d_btab_v = nullptr;
+  int2* d_btab_t = nullptr;
+  Counters* d_ctr = nullptr;
+  int* d_flag = nullptr;
+  double* d_energy = nullptr;
+  double* d_stage = nullptr;
+  size_t stage_elems = 0;
+  void* d_flush = nullptr;
+  size_t flush_bytes = 0;
+  Ops<double> ops_d{};
+  Ops<float> ops_f{};
+  int block = 256;
+  int blocks_v = 0, blocks_t = 0;
+  bool multi = false;
+  int graph_steps = 100;
+  cudaGraphExec_t graph = nullptr;
+  int graph_block = 0;
+  long t = 0;
+  long max_steps = 0;
+  int watchdog_every = 0;
+  dg_gpu_stats stats{};
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  ~dg_gpu_ctx() {
+    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (void* p : allocs) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  template <class T> int alloc(T** out, size_t count) {
+    void* p = nullptr;
+    if (count == 0) count = 1;
+    CK(cudaMalloc(&p, count * sizeof(T)));
+    allocs.push_back(p);
+    *out = (T*)p;
+    return DG_OK;
+  }
+  template <class T> int upload(T** out, const std::vector<T>& h) {
+    int rc = alloc(out, h.size());
+    if (rc) return rc;
+    if (!h.empty()) CK(cudaMemcpyAsync(*out, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    return DG_OK;
+  }
+};
+
+namespace {
+
+constexpr long long P2_IBE[9] = {6, 4, 1, 1, 2, 3, 6, 5, 3};
+
+// Per-mesh host preparation shared by both arithmetic types.
+struct Prepared {
+  long K;
+  int Kp, S, n_rec;
+  std::vector<int> order;       // internal -> caller element
+  std::vector<int> new_of_old;  // caller -> internal
+  std::vector<double> geo;      // [Kp][4] rx sx rz sz
+  std::vector<double> mat;      // [Kp][4] 1/rho lambda mu lambda+2mu
+  std::vector<int4> face;       // [Kp]
+  std::vector<double> sponge;   // [6][Kp]
+  std::vector<int> src_elem;
+  std::vector<double> src_fun;  // [S][6]
+  std::vector<int> rec_elem, rec_node;
+  std::vector<double> Dx, Dz, Q, AB;  // SoA, reference path only
+  long sponge_elems = 0;
+};
+
+int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
+  if (m.K <= 0 || m.K > (1L << 26)) return fail(DG_ERR_ARG, "K must be in [1, 2^26]");
+  if (m.Np != 6 || m.Nfp != 3) return fail(DG_ERR_UNSUPPORTED, "only P2 (Np = 6, Nfp = 3) is supported");
+  if (!m.Point || !m.Triangle || m.n_points <= 0 || !m.Vr || !m.Vs || !m.inverV || !m.S || !m.ibe || !m.Neighbor ||
+      !m.Node_Neighbor || !m.Edge_flag || !m.A || !m.B || !m.absorb_fun || !m.wavelet || m.n_steps <= 0)
+    return fail(DG_ERR_ARG, "missing mesh array");
+  if (m.n_shots < 1 || !m.source || !m.fun) return fail(DG_ERR_ARG, "need at least one shot with source and fun");
+  if (m.n_rec < 0 || (m.n_rec > 0 && !m.receiver)) return fail(DG_ERR_ARG, "bad receivers");
+  if (!(m.dt > 0) || !std::isfinite(m.dt)) return fail(DG_ERR_ARG, "dt must be positive and finite");
+  if (precision == DG_FP64_REF && (!m.Dx || !m.Dz || !m.Q))
+    return fail(DG_ERR_ARG, "DG_FP64_REF needs the reference's Dx, Dz and Q");
+  for (int q = 0; q < 9; q++)
+    if (m.ibe[q] != P2_IBE[q]) return fail(DG_ERR_UNSUPPORTED, "ibe is not the P2 face table {6,4,1},{1,2,3},{6,5,3}");
+  if ((long long)m.n_shots * m.K > (1LL << 31) - 1) return fail(DG_ERR_ARG, "K * n_shots too large");
+
+  const long K = m.K;
+  p.K = K;
+  p.S = m.n_shots;
+  p.n_rec = m.n_rec;
+  p.Kp = (int)((K + 31) / 32 * 32);
+  const int Kp = p.Kp;
+
+  // geometry per caller element, as Dx_Dz (fun_DG.c:1150-1165)
+  std::vector<double> cx(K), cz(K), rxa(K * 4);
+  for (long e = 0; e < K; e++) {
+    double X[3], Z[3];
+    for (int v = 0; v < 3; v++) {
+      long pt = m.Triangle[e * 3 + v] - 1;
+      if (pt < 0 || pt >= m.n_points) return fail(DG_ERR_MESH, "Triangle holds a vertex index out of range");
+      X[v] = m.Point[pt * 2 + 0];
+      Z[v] = m.Point[pt * 2 + 1];
+    }
+    const double Xr = (X[1] - X[0]) * 0.5, Zr = (Z[1] - Z[0]) * 0.5;
+    const double Xs = (X[2] - X[0]) * 0.5, Zs = (Z[2] - Z[0]) * 0.5;
+    const double J = Xr * Zs - Xs * Zr;
+    if (!(J > 0) && precision != DG_FP64_REF)
+      return fail(DG_ERR_ORIENTATION, "a triangle is not counter-clockwise (Jacobian <= 0)");
+    rxa[e * 4 + 0] = Zs / J;
+    rxa[e * 4 + 1] = -Zr / J;
+    rxa[e * 4 + 2] = -Xs / J;
+    rxa[e * 4 + 3] = Xr / J;
+    cx[e] = (X[0] + X[1] + X[2]) / 3.0;
+    cz[e] = (Z[0] + Z[1] + Z[2]) / 3.0;
+  }
+
+  // locality order
+  p.order.resize(K);
+  for (long e = 0; e < K; e++) p.order[e] = (int)e;
+  if (reorder) {
+    double x0 = cx[0], x1 = cx[0], z0 = cz[0], z1 = cz[0];
+    for (long e = 0; e < K; e++) {
+      x0 = std::min(x0, cx[e]); x1 = std::max(x1, cx[e]);
+      z0 = std::min(z0, cz[e]); z1 = std::max(z1, cz[e]);
+    }
+    const double span = std::max(x1 - x0, z1 - z0) + 1e-300;
+    std::vector<std::pair<uint64_t, int>> key(K);
+    for (long e = 0; e < K; e++) {
+      uint32_t ix = (uint32_t)std::min(65535.0, std::floor((cx[e] - x0) / span * 65535.0));
+      uint32_t iz = (uint32_t)std::min(65535.0, std::floor((cz[e] - z0) / span * 65535.0));
+      key[e] = {hilbert(ix, iz), (int)e};
+    }
+    std::sort(key.begin(), key.end());
+    for (long e = 0; e < K; e++) p.order[e] = key[e].second;
+  }
+  p.new_of_old.assign(K, 0);
+  for (long n = 0; n < K; n++) p.new_of_old[p.order[n]] = (int)n;
+
+  // sponge flags
+  std::vector<char> in_sponge(K, 0);
+  for (long e = 0; e < K; e++)
+    for (int i = 0; i < 6; i++)
+      if (m.absorb_fun[e * 6 + i] != 1.0) in_sponge[e] = 1;
+
+  p.geo.assign((size_t)Kp * 4, 0.0);
+  p.mat.assign((size_t)Kp * 4, 0.0);
+  p.face.assign(Kp, make_int4(-1, -1, -1, 0));
+  p.sponge.assign((size_t)6 * Kp, 1.0);
+  for (long n = 0; n < K; n++) {
+    const long e = p.order[n];
+    for (int c = 0; c < 4; c++) p.geo[n * 4 + c] = rxa[e * 4 + c];
+    const double* A = m.A + e * 5;
+    const double* B = m.B + e * 5;
+    if (precision != DG_FP64_REF) {
+      // the geometric-factor form relies on Elastic_A_B's structure (fun_DG.c:1076-1086)
+      if (!(A[0] == A[1] && A[0] == B[0] && A[0] == B[1] && A[2] == B[3] && A[3] == B[2] && A[4] == B[4]))
+        return fail(DG_ERR_MESH, "A/B do not have the structure Elastic_A_B produces");
+    }
+    p.mat[n * 4 + 0] = A[0];
+    p.mat[n * 4 + 1] = A[3];
+    p.mat[n * 4 + 2] = A[4];
+    p.mat[n * 4 + 3] = A[2];
+    int codes[3];
+    for (int f = 0; f < 3; f++) {
+      const long flag = m.Edge_flag[e * 3 + f];
+      const long nb = m.Neighbor[e * 3 + f] - 1;
+      if (nb < 0 || nb >= K) return fail(DG_ERR_MESH, "Neighbor holds an index out of range");
+      if (flag == 0) { codes[f] = -1; continue; }
+      if (flag != 1) return fail(DG_ERR_MESH, "Edge_flag must be 0 or 1");
+      const long* nn = m.Node_Neighbor + e * 9 + f * 3;
+      int found = -1;
+      for (int g = 0; g < 3 && found < 0; g++) {
+        bool same = true, rev = true;
+        for (int k = 0; k < 3; k++) {
+          same &= nn[k] == P2_IBE[g * 3 + k];
+          rev &= nn[k] == P2_IBE[g * 3 + 2 - k];
+        }
+        if (same) found = g * 2;
+        else if (rev) found = g * 2 + 1;
+      }
+      if (found < 0) return fail(DG_ERR_MESH, "Node_Neighbor is not a P2 face of the neighbour");
+      codes[f] = (p.new_of_old[nb] << 4) | (in_sponge[nb] ? 8 : 0) | ((found >> 1) << 1) | (found & 1);
+    }
+    p.face[n] = make_int4(codes[0], codes[1], codes[2], in_sponge[e] ? 1 : 0);
+    if (in_sponge[e]) {
+      p.sponge_elems++;
+      for (int i = 0; i < 6; i++) p.sponge[(size_t)i * Kp + n] = m.absorb_fun[e * 6 + i];
+    }
+  }
+  p.src_elem.resize(p.S);
+  p.src_fun.resize((size_t)p.S * 6);
+  for (int s = 0; s < p.S; s++) {
+    const long tri = m.source[s * 2 + 0] - 1, node = m.source[s * 2 + 1] - 1;
+    if (tri < 0 || tri >= K || node < 0 || node >= 6) return fail(DG_ERR_MESH, "source out of range");
+    p.src_elem[s] = p.new_of_old[tri];
+    for (int i = 0; i < 6; i++) p.src_fun[s * 6 + i] = m.fun[s * 6 + i];
+  }
+  p.rec_elem.resize(p.n_rec);
+  p.rec_node.resize(p.n_rec);
+  for (int r = 0; r < p.n_rec; r++) {
+    const long tri = m.receiver[r * 2 + 0] - 1, node = m.receiver[r * 2 + 1] - 1;
+    if (tri < 0 || tri >= K || node < 0 || node >= 6) return fail(DG_ERR_MESH, "receiver out of range");
+    p.rec_elem[r] = p.new_of_old[tri];
+    p.rec_node[r] = (int)node;
+  }
+  if (precision == DG_FP64_REF) {
+    p.Dx.assign((size_t)36 * Kp, 0.0);
+    p.Dz.assign((size_t)36 * Kp, 0.0);
+    p.Q.assign((size_t)30 * Kp, 0.0);
+    p.AB.assign((size_t)10 * Kp, 0.0);
+    for (long n = 0; n < K; n++) {
+      const long e = p.order[n];
+      for (int q = 0; q < 36; q++) {
+        p.Dx[(size_t)q * Kp + n] = m.Dx[e * 36 + q];
+        p.Dz[(size_t)q * Kp + n] = m.Dz[e * 36 + q];
+      }
+      for (int q = 0; q < 30; q++) p.Q[(size_t)q * Kp + n] = m.Q[e * 30 + q];
+      for (int q = 0; q < 5; q++) {
+        p.AB[(size_t)q * Kp + n] = m.A[e * 5 + q];
+        p.AB[(size_t)(5 + q) * Kp + n] = m.B[e * 5 + q];
+      }
+    }
+  }
+  return DG_OK;
+}
+
+template <class R> std::vector<R> cast(const std::vector<double>& v) { return std::vector<R>(v.begin(), v.end()); }
+
+template <class R>
+int upload_mesh(dg_gpu_ctx* c, const dg_gpu_mesh& m, Prepared& p, MeshDev<R>& d) {
+  using R4 = typename R4T<R>::type;
+  int rc;
+  memset(&d, 0, sizeof d);
+  d.K = (int)p.K;
+  d.Kp = p.Kp;
+  d.S = p.S;
+  d.n_rec = p.n_rec;
+  d.P = (long long)p.Kp * p.S;
+  d.steps = m.n_steps;
+  d.dt = (R)m.dt;
+  d.sponge_elems = (int)p.sponge_elems;
+  if ((rc = c->alloc(&d.U, (size_t)NPLANES * d.P))) return rc;
+  CK(cudaMemsetAsync(d.U, 0, sizeof(R) * NPLANES * d.P, c->stream));
+  if (c->kahan) {
+    if ((rc = c->alloc(&d.C, (size_t)NPLANES * d.P))) return rc;
+    CK(cudaMemsetAsync(d.C, 0, sizeof(R) * NPLANES * d.P, c->stream));
+  }
+  std::vector<R4> geo(p.Kp), mat(p.Kp);
+  for (int n = 0; n < p.Kp; n++) {
+    geo[n] = {(R)p.geo[n * 4 + 0], (R)p.geo[n * 4 + 1], (R)p.geo[n * 4 + 2], (R)p.geo[n * 4 + 3]};
+    mat[n] = {(R)p.mat[n * 4 + 0], (R)p.mat[n * 4 + 1], (R)p.mat[n * 4 + 2], (R)p.mat[n * 4 + 3]};
+  }
+  R4* g4;
+  R4* m4;
+  if ((rc = c->upload(&g4, geo))) return rc;
+  if ((rc = c->upload(&m4, mat))) return rc;
+  d.geo = g4;
+  d.mat = m4;
+  int4* f4;
+  if ((rc = c->upload(&f4, p.face))) return rc;
+  d.face = f4;
+  R* sp;
+  if ((rc = c->upload(&sp, cast<R>(p.sponge)))) return rc;
+  d.sponge = sp;
+  double* wv;
+  if ((rc = c->upload(&wv, std::vector<double>(m.wavelet, m.wavelet + m.n_steps)))) return rc;
+  d.wavelet = wv;
+  int* se;
+  if ((rc = c->upload(&se, p.src_elem))) return rc;
+  d.src_elem = se;
+  R* sf;
+  if ((rc = c->upload(&sf, cast<R>(p.src_fun)))) return rc;
+  d.src_fun = sf;
+  int *re, *rn;
+  if ((rc = c->upload(&re, p.rec_elem))) return rc;
+  if ((rc = c->upload(&rn, p.rec_node))) return rc;
+  d.rec_elem = re;
+  d.rec_node = rn;
+  const size_t trace_elems = (size_t)m.n_steps * 2 * std::max(1, p.n_rec) * p.S;
+  if ((rc = c->alloc(&d.trace, trace_elems))) return rc;
+  CK(cudaMemsetAsync(d.trace, 0, sizeof(R) * trace_elems, c->stream));
+  if (c->precision == DG_FP64_REF) {
+    double *dx, *dz, *q, *ab;
+    if ((rc = c->upload(&dx, p.Dx))) return rc;
+    if ((rc = c->upload(&dz, p.Dz))) return rc;
+    if ((rc = c->upload(&q, p.Q))) return rc;
+    if ((rc = c->upload(&ab, p.AB))) return rc;
+    d.Dx = dx;
+    d.Dz = dz;
+    d.Q = q;
+    d.AB = ab;
+  }
+  return DG_OK;
+}
+
+template <class R> void fill_ops(Ops<R>& o, const dg_gpu_mesh& m) {
+  // Dr = Vr inv(V), Ds = Vs inv(V) from the parsed operator files
+  for (int i = 0; i < 6; i++)
+    for (int q = 0; q < 6; q++) {
+      double a = 0, b = 0;
+      for (int k = 0; k < 6; k++) {
+        a += m.Vr[i * 6 + k] * m.inverV[k * 6 + q];
+        b += m.Vs[i * 6 + k] * m.inverV[k * 6 + q];
+      }
+      o.Dr[i * 6 + q] = (R)a;
+      o.Ds[i * 6 + q] = (R)b;
+    }
+  for (int q = 0; q < 54; q++) o.L[q] = (R)m.S[q];
+  // reference mass matrix inv(V V^T) = inverV^T inverV
+  for (int i = 0; i < 6; i++)
+    for (int k = 0; k < 6; k++) {
+      double a = 0;
+      for (int q = 0; q < 6; q++) a += m.inverV[q * 6 + i] * m.inverV[q * 6 + k];
+      o.M[i * 6 + k] = (R)a;
+    }
+}
+
+// grid and block tables for the current block size
+template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDev<R>** d_tab) {
+  const int B = c->block;
+  std::vector<int2> bv, bt;
+  for (size_t k = 0; k < md.size(); k++) {
+    MeshHostInfo& h = c->mi[k];
+    h.elem_blocks = (int)(((long long)h.K * h.S + B - 1) / B);
+    h.rec_blocks = (h.n_rec * h.S + B - 1) / B;
+    md[k].n_elem_blocks = h.elem_blocks;
+    for (int b = 0; b < h.elem_blocks; b++) bv.push_back(make_int2((int)k, b));
+    for (int b = 0; b < h.elem_blocks + h.rec_blocks; b++) bt.push_back(make_int2((int)k, b));
+  }
+  c->blocks_v = (int)bv.size();
+  c->blocks_t = (int)bt.size();
+  if (c->multi) {
+    if (!*d_tab) {
+      int rc = c->alloc(d_tab, md.size());
+      if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(*d_tab, md.data(), md.size() * sizeof(MeshDev<R>), cudaMemcpyHostToDevice, c->stream));
+    // block tables are rebuilt for each block size; old ones stay allocated until free
+    int rc = c->upload(&c->d_btab_v, bv);
+    if (rc) return rc;
+    rc = c->upload(&c->d_btab_t, bt);
+    if (rc) return rc;
+  }
+  return DG_OK;
+}
+
+int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid = nullptr, cudaEvent_t after = nullptr) {
+  const dim3 bl(c->block);
+  const dim3 gv(c->blocks_v), gt(c->blocks_t);
+  cudaStream_t st = c->stream;
+  if (before_t) CK(cudaEventRecord(before_t, st));
+  if (c->precision == DG_FP64_REF) {
+    if (c->multi) {
+      k_velocity_ref<true><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress_ref<true><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
+    } else {
+      k_velocity_ref<false><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress_ref<false><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
+    }
+  } else if (c->is_double) {
+    if (c->multi) {
+      k_velocity<double, false, true><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress<double, false, true><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
+    } else {
+      k_velocity<double, false, false><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress<double, false, false><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
+    }
+  } else if (c->kahan) {
+    if (c->multi) {
+      k_velocity<float, true, true><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress<float, true, true><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_t, c->d_ctr);
+    } else {
+      k_velocity<float, true, false><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress<float, true, false><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
+    }
+  } else {
+    if (c->multi) {
+      k_velocity<float, false, true><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress<float, false, true><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_t, c->d_ctr);
+    } else {
+      k_velocity<float, false, false><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress<float, false, false><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
+    }
+  }
+  CK(cudaGetLastError());
+  if (after) CK(cudaEventRecord(after, st));
+  return DG_OK;
+}
+
+int rebuild_graph(dg_gpu_ctx* c) {
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  if (c->graph_steps <= 0) return DG_OK;
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = DG_OK;
+  for (int k = 0; k < c->graph_steps && rc == DG_OK; k++) rc = launch_step(c);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __LINE__);
+  e = cudaGraphInstantiate(&c->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __LINE__);
+  c->graph_block = c->block;
+  return DG_OK;
+}
+
+int set_block(dg_gpu_ctx* c, int block) {
+  c->block = block;
+  int rc = c->is_double ? layout(c, c->md_d, &c->d_tab_d) : layout(c, c->md_f, &c->d_tab_f);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
+int zero_state(dg_gpu_ctx* c) {
+  for (size_t k = 0; k < c->mi.size(); k++) {
+    const MeshHostInfo& h = c->mi[k];
+    const size_t esz = c->is_double ? 8 : 4;
+    void* U = c->is_double ? (void*)c->md_d[k].U : (void*)c->md_f[k].U;
+    void* C = c->is_double ? (void*)c->md_d[k].C : (void*)c->md_f[k].C;
+    void* T = c->is_double ? (void*)c->md_d[k].trace : (void*)c->md_f[k].trace;
+    const size_t P = (size_t)h.Kp * h.S;
+    CK(cudaMemsetAsync(U, 0, esz * NPLANES * P, c->stream));
+    if (C) CK(cudaMemsetAsync(C, 0, esz * NPLANES * P, c->stream));
+    CK(cudaMemsetAsync(T, 0, esz * (size_t)h.steps * 2 * std::max(1, h.n_rec) * h.S, c->stream));
+  }
+  CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->t = 0;
+  return DG_OK;
+}
+
+int autotune(dg_gpu_ctx* c, const char* cache) {
+  char key[256];
+  long long sumK = 0, sumKS = 0;
+  for (auto& h : c->mi) { sumK += h.K; sumKS += (long long)h.K * h.S; }
+  snprintf(key, sizeof key, "p%d_m%zu_K%lld_KS%lld", c->precision, c->mi.size(), sumK, sumKS);
+  if (cache) {
+    FILE* f = fopen(cache, "r");
+    if (f) {
+      char k2[256];
+      int b;
+      while (fscanf(f, "%255s %d", k2, &b) == 2)
+        if (!strcmp(k2, key) && (b == 64 || b == 128 || b == 256)) {
+          fclose(f);
+          return set_block(c, b);
+        }
+      fclose(f);
+    }
+  }
+  const int cand[3] = {64, 128, 256};
+  const long probe = std::min<long>(8, c->max_steps);
+  float best = 1e30f;
+  int best_b = 256;
+  for (int b : cand) {
+    int rc = set_block(c, b);
+    if (rc) return rc;
+    for (int w = 0; w < 2 && w < probe; w++)
+      if ((rc = launch_step(c))) return rc;
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    for (long k = 2; k < probe; k++)
+      if ((rc = launch_step(c))) return rc;
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(cudaEventSynchronize(c->ev[1]));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+    if (ms < best) { best = ms; best_b = b; }
+    if ((rc = zero_state(c))) return rc;
+  }
+  if (cache) {
+    FILE* f = fopen(cache, "a");
+    if (f) { fprintf(f, "%s %d\n", key, best_b); fclose(f); }
+  }
+  return set_block(c, best_b);
+}
+
+}  // namespace
+
+extern "C" {
+
+void dg_gpu_default_opts(dg_gpu_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof *o);
+  o->precision = DG_FP64;
+  o->device = 0;
+  o->reorder = 1;
+  o->block_threads = 0;
+  o->graph_steps = 0;
+  o->autotune = 0;
+  o->watchdog_every = 0;
+  o->tune_cache = nullptr;
+}
+
+const char* dg_gpu_strerror(int code) {
+  switch (code) {
+    case DG_OK: return "ok";
+    case DG_ERR_ARG: return "invalid argument";
+    case DG_ERR_CUDA: return "CUDA error";
+    case DG_ERR_NOMEM: return "out of memory";
+    case DG_ERR_MESH: return "inconsistent mesh arrays";
+    case DG_ERR_NONFINITE: return "non-finite values in the wave field";
+    case DG_ERR_STATE: return "invalid call for the current state";
+    case DG_ERR_UNSUPPORTED: return "unsupported configuration";
+    case DG_ERR_NODEVICE: return "no usable sm_100 CUDA device";
+    case DG_ERR_ORIENTATION: return "triangle with non-positive Jacobian";
+    default: return "unknown error";
+  }
+}
+
+const char* dg_gpu_last_error(void) { return g_last.c_str(); }
+
+int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const dg_gpu_opts* opts_in) {
+  if (!out) return fail(DG_ERR_ARG, "ctx pointer is null");
+  *out = nullptr;
+  if (!meshes || n_meshes < 1) return fail(DG_ERR_ARG, "need at least one mesh");
+  if (n_meshes > DG_MAX_MESHES) return fail(DG_ERR_UNSUPPORTED, "too many meshes");
+  dg_gpu_opts o;
+  if (opts_in) o = *opts_in; else dg_gpu_default_opts(&o);
+  if (o.precision < DG_FP64_REF || o.precision > DG_FP32_KAHAN) return fail(DG_ERR_ARG, "unknown precision");
+  if (o.block_threads != 0 && o.block_threads != 64 && o.block_threads != 128 && o.block_threads != 256)
+    return fail(DG_ERR_ARG, "block_threads must be 0, 64, 128 or 256");
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0)
+    return fail(DG_ERR_NODEVICE, "no CUDA device with that ordinal");
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, o.device));
+  if (prop.major != 10) return fail(DG_ERR_NODEVICE, "the engine is built for sm_100a (B200)");
+  CK(cudaSetDevice(o.device));
+
+  std::unique_ptr<dg_gpu_ctx> c(new dg_gpu_ctx());
+  c->device = o.device;
+  c->precision = o.precision;
+  c->is_double = o.precision == DG_FP64_REF || o.precision == DG_FP64;
+  c->kahan = o.precision == DG_FP32_KAHAN;
+  c->multi = n_meshes > 1;
+  c->watchdog_every = std::max(0, o.watchdog_every);
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (auto& e : c->ev) CK(cudaEventCreate(&e));
+
+  c->mi.resize(n_meshes);
+  double bytes = 0, dof = 0;
+  size_t stage = 1;
+  const size_t w = c->is_double ? 8 : 4;
+  for (int k = 0; k < n_meshes; k++) {
+    Prepared p;
+    int rc = prepare(meshes[k], o.precision, o.reorder, p);
+    if (rc) return rc;
+    MeshHostInfo& h = c->mi[k];
+    h.K = p.K;
+    h.Kp = p.Kp;
+    h.S = p.S;
+    h.n_rec = p.n_rec;
+    h.steps = meshes[k].n_steps;
+    h.dt = meshes[k].dt;
+    h.new_of_old = p.new_of_old;
+    h.sponge_elems = p.sponge_elems;
+    if ((rc = c->upload(&h.d_new_of_old, p.new_of_old))) return rc;
+    if (c->is_double) {
+      c->md_d.emplace_back();
+      if ((rc = upload_mesh<double>(c.get(), meshes[k], p, c->md_d.back()))) return rc;
+    } else {
+      c->md_f.emplace_back();
+      if ((rc = upload_mesh<float>(c.get(), meshes[k], p, c->md_f.back()))) return rc;
+    }
+    c->max_steps = std::max(c->max_steps, h.steps);
+    // algorithmic bytes per step: 90 state values (+60 compensation values) per element and shot,
+    // plus per element geo + mat (2 x 4 values) and face codes (2 x 16 B) over the two half-steps
+    double per = 90.0 * h.S * w + (c->kahan ? 60.0 * h.S * 4 : 0.0) + 16.0 * w + 32.0;
+    if (o.precision == DG_FP64_REF) per = 90.0 * h.S * 8 + 2.0 * 72 * 8 + 30 * 8 + 10 * 8 + 32.0;
+    bytes += per * (double)h.K;
+    dof += 30.0 * (double)h.K * h.S;
+    stage = std::max(stage, (size_t)std::max<long>(h.K * 6, h.steps * std::max(1, h.n_rec)));
+  }
+  c->stats.bytes_per_step = bytes;
+  c->stats.dof_per_step = dof;
+  if (c->is_double) fill_ops(c->ops_d, meshes[0]); else fill_ops(c->ops_f, meshes[0]);
+  int rc;
+  if ((rc = c->alloc(&c->d_ctr, 1))) return rc;
+  if ((rc = c->alloc(&c->d_flag, 1))) return rc;
+  if ((rc = c->alloc(&c->d_energy, 1))) return rc;
+  if ((rc = c->alloc(&c->d_stage, stage))) return rc;
+  c->stage_elems = stage;
+  CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), c->stream));
+
+  int block = o.block_threads ? o.block_threads : 256;
+  if ((rc = set_block(c.get(), block))) return rc;
+  if (o.autotune && !o.block_threads)
+    if ((rc = autotune(c.get(), o.tune_cache))) return rc;
+  c->graph_steps = o.graph_steps < 0 ? 0 : (o.graph_steps ? o.graph_steps : (int)std::min<long>(100, c->max_steps));
+  if ((rc = rebuild_graph(c.get()))) return rc;
+  if ((rc = zero_state(c.get()))) return rc;
+  c->stats.block_threads = c->block;
+  c->stats.graph_steps = c->graph_steps;
+  *out = c.release();
+  return DG_OK;
+}
+
+static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
+  if (!c || n < 0) return fail(DG_ERR_ARG, "bad arguments");
+  if (c->t + n > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
+  CK(cudaSetDevice(c->device));
+  c->stats.launches = 0;
+  if (timed) { c->stats.ms_velocity = 0; c->stats.ms_stress = 0; }
+  long done = 0;
+  while (done < n) {
+    long chunk = n - done;
+    if (c->watchdog_every > 0) {
+      long to_check = c->watchdog_every - (c->t % c->watchdog_every);
+      chunk = std::min(chunk, to_check);
+    }
+    if (timed) {
+      for (long k = 0; k < chunk; k++) {
+        int rc = launch_step(c, c->ev[0], c->ev[1], c->ev[2]);
+        if (rc) return rc;
+        CK(cudaEventSynchronize(c->ev[2]));
+        float a = 0, b = 0;
+        CK(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
+        CK(cudaEventElapsedTime(&b, c->ev[1], c->ev[2]));
+        c->stats.ms_velocity += a;
+        c->stats.ms_stress += b;
+      }
+      c->stats.launches += 2 * chunk;
+    } else {
+      long k = 0;
+      if (c->graph && c->graph_steps > 0)
+        for (; k + c->graph_steps <= chunk; k += c->graph_steps) CK(cudaGraphLaunch(c->graph, c->stream));
+      for (; k < chunk; k++) {
+        int rc = launch_step(c);
+        if (rc) return rc;
+      }
+      c->stats.launches += 2 * chunk;
+    }
+    done += chunk;
+    c->t += chunk;
+    if (c->watchdog_every > 0 && c->t % c->watchdog_every == 0) {
+      CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
+      for (size_t k = 0; k < c->mi.size(); k++) {
+        const long long nvals = 12LL * c->mi[k].Kp * c->mi[k].S;
+        if (c->is_double) k_nonfinite<double><<<592, 256, 0, c->stream>>>(c->md_d[k].U, nvals, c->d_flag);
+        else k_nonfinite<float><<<592, 256, 0, c->stream>>>(c->md_f[k].U, nvals, c->d_flag);
+        c->stats.launches++;
+      }
+      int flag = 0;
+      CK(cudaMemcpyAsync(&flag, c->d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (flag) return fail(DG_ERR_NONFINITE, "NaN or Inf in the velocity fields");
+    }
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  c->stats.steps_done = c->t;
+  return DG_OK;
+}
+
+int dg_gpu_step(dg_gpu_ctx* c, long n) { return do_steps(c, n, false); }
+int dg_gpu_step_timed(dg_gpu_ctx* c, long n) { return do_steps(c, n, true); }
+
+int dg_gpu_fetch(dg_gpu_ctx* c, int what, int mesh, int shot, double* dst) {
+  if (!c || !dst || mesh < 0 || mesh >= (int)c->mi.size()) return fail(DG_ERR_ARG, "bad arguments");
+  const MeshHostInfo& h = c->mi[mesh];
+  if (shot < 0 || shot >= h.S) return fail(DG_ERR_ARG, "shot out of range");
+  CK(cudaSetDevice(c->device));
+  const int B = 256;
+  if (what >= DG_VX && what <= DG_TXZ) {
+    const long long n = h.K * 6;
+    const int grid = (int)((n + B - 1) / B);
+    if (c->is_double)
+      k_fetch_field<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].U, what * 6, c->md_d[mesh].P, h.S, shot,
+                                                       h.d_new_of_old, (int)h.K, c->d_stage);
+    else
+      k_fetch_field<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].U, what * 6, c->md_f[mesh].P, h.S, shot,
+                                                      h.d_new_of_old, (int)h.K, c->d_stage);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst, c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  } else if (what == DG_TRACE_X || what == DG_TRACE_Z) {
+    const long long steps = std::min(c->t, h.steps);
+    const long long n = steps * h.n_rec;
+    if (n > 0) {
+      const int grid = (int)((n + B - 1) / B);
+      const int comp = what - DG_TRACE_X;
+      if (c->is_double)
+        k_fetch_trace<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].trace, comp, h.n_rec, h.S, shot, steps, c->d_stage);
+      else
+        k_fetch_trace<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].trace, comp, h.n_rec, h.S, shot, steps, c->d_stage);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(dst, c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+  } else if (what == DG_ENERGY) {
+    CK(cudaMemsetAsync(c->d_energy, 0, sizeof(double), c->stream));
+    const int grid = (int)((h.K + B - 1) / B);
+    if (c->is_double) k_energy<double><<<grid, B, 0, c->stream>>>(c->ops_d, c->md_d[mesh], shot, c->d_energy);
+    else k_energy<float><<<grid, B, 0, c->stream>>>(c->ops_f, c->md_f[mesh], shot, c->d_energy);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst, c->d_energy, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    return fail(DG_ERR_STATE, "unknown fetch item");
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
+int dg_gpu_load(dg_gpu_ctx* c, int what, int mesh, int shot, const double* src) {
+  if (!c || !src || mesh < 0 || mesh >= (int)c->mi.size()) return fail(DG_ERR_ARG, "bad arguments");
+  const MeshHostInfo& h = c->mi[mesh];
+  if (shot < 0 || shot >= h.S) return fail(DG_ERR_ARG, "shot out of range");
+  if (what < DG_VX || what > DG_TXZ) return fail(DG_ERR_STATE, "only fields can be loaded");
+  CK(cudaSetDevice(c->device));
+  const long long n = h.K * 6;
+  CK(cudaMemcpyAsync(c->d_stage, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  const int B = 256, grid = (int)((n + B - 1) / B);
+  if (c->is_double)
+    k_load_field<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].U, c->md_d[mesh].C, what * 6, c->md_d[mesh].P, h.S,
+                                                    shot, h.d_new_of_old, (int)h.K, c->d_stage);
+  else
+    k_load_field<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].U, c->md_f[mesh].C, what * 6, c->md_f[mesh].P, h.S,
+                                                   shot, h.d_new_of_old, (int)h.K, c->d_stage);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
+int dg_gpu_reset(dg_gpu_ctx* c) {
+  if (!c) return fail(DG_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  return zero_state(c);
+}
+
+int dg_gpu_set_wavelet(dg_gpu_ctx* c, int mesh, long t0, long n, const double* w) {
+  if (!c || !w || mesh < 0 || mesh >= (int)c->mi.size() || t0 < 0 || n < 0 || t0 + n > c->mi[mesh].steps)
+    return fail(DG_ERR_ARG, "bad arguments");
+  CK(cudaSetDevice(c->device));
+  const double* dw = c->is_double ? c->md_d[mesh].wavelet : c->md_f[mesh].wavelet;
+  CK(cudaMemcpyAsync((void*)(dw + t0), w, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
+int dg_gpu_flush_l2(dg_gpu_ctx* c) {
+  if (!c) return fail(DG_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  if (!c->d_flush) {
+    c->flush_bytes = (size_t)256 << 20;
+    void* p = nullptr;
+    CK(cudaMalloc(&p, c->flush_bytes));
+    c->allocs.push_back(p);
+    c->d_flush = p;
+  }
+  CK(cudaMemsetAsync(c->d_flush, (int)(c->t & 0xff), c->flush_bytes, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
+int dg_gpu_stats_get(dg_gpu_ctx* c, dg_gpu_stats* out) {
+  if (!c || !out) return fail(DG_ERR_ARG, "bad arguments");
+  c->stats.steps_done = c->t;
+  c->stats.block_threads = c->block;
+  c->stats.graph_steps = c->graph_steps;
+  *out = c->stats;
+  return DG_OK;
+}
+
+long dg_gpu_steps_done(dg_gpu_ctx* c) { return c ? c->t : -1; }
+
+int dg_gpu_free(dg_gpu_ctx* c) {
+  if (!c) return DG_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  delete c;
+  return DG_OK;
+}
+
+}  // extern "C"

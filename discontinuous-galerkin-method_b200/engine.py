@@ -1,0 +1,232 @@
+"""ctypes binding of the sm_100a engine (csrc/dg_gpu.cu, include/dg_gpu.h).
+
+``Engine`` mirrors the reference's per-step call sequence (DG_leap_Frog_OpenMP.c:418-437):
+``step(n)`` advances every mesh n steps (sponge, source, velocity, stress, record),
+``fetch`` returns fields/traces in the reference's element-major layout.  There is no CPU
+fallback: a missing library or device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import build as _build
+
+FP64_REF, FP64, FP32, FP32_KAHAN = 0, 1, 2, 3
+PRECISIONS = {"fp64_ref": FP64_REF, "fp64": FP64, "fp32": FP32, "fp32_kahan": FP32_KAHAN}
+VX, VZ, TXX, TZZ, TXZ, TRACE_X, TRACE_Z, ENERGY = range(8)
+FIELDS = {"Vx": VX, "Vz": VZ, "Txx": TXX, "Tzz": TZZ, "Txz": TXZ}
+
+ERRORS = {0: "DG_OK", -1: "DG_ERR_ARG", -2: "DG_ERR_CUDA", -3: "DG_ERR_NOMEM", -4: "DG_ERR_MESH",
+          -5: "DG_ERR_NONFINITE", -6: "DG_ERR_STATE", -7: "DG_ERR_UNSUPPORTED", -8: "DG_ERR_NODEVICE",
+          -9: "DG_ERR_ORIENTATION"}
+
+# exported symbols of include/dg_gpu.h (checked by the CPU tests)
+EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_timed", "dg_gpu_fetch", "dg_gpu_load",
+           "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_steps_done",
+           "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error"]
+
+
+class DGError(RuntimeError):
+    def __init__(self, code, where, detail=""):
+        self.code = code
+        super().__init__("%s failed: %s (%d) %s" % (where, ERRORS.get(code, "?"), code, detail))
+
+
+class _Mesh(C.Structure):
+    _fields_ = [("K", C.c_long), ("Np", C.c_int), ("Nfp", C.c_int), ("n_points", C.c_long),
+                ("Point", C.c_void_p), ("Triangle", C.c_void_p), ("Vr", C.c_void_p), ("Vs", C.c_void_p),
+                ("inverV", C.c_void_p), ("V", C.c_void_p), ("S", C.c_void_p), ("ibe", C.c_void_p),
+                ("Neighbor", C.c_void_p), ("Node_Neighbor", C.c_void_p), ("Edge_flag", C.c_void_p),
+                ("A", C.c_void_p), ("B", C.c_void_p), ("Dx", C.c_void_p), ("Dz", C.c_void_p), ("Q", C.c_void_p),
+                ("absorb_fun", C.c_void_p), ("n_shots", C.c_int), ("source", C.c_void_p), ("fun", C.c_void_p),
+                ("n_rec", C.c_int), ("receiver", C.c_void_p), ("dt", C.c_double), ("n_steps", C.c_long),
+                ("wavelet", C.c_void_p)]
+
+
+class _Opts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("device", C.c_int), ("reorder", C.c_int), ("block_threads", C.c_int),
+                ("graph_steps", C.c_int), ("autotune", C.c_int), ("watchdog_every", C.c_int),
+                ("tune_cache", C.c_char_p)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("ms_velocity", C.c_double), ("ms_stress", C.c_double), ("launches", C.c_long),
+                ("steps_done", C.c_long), ("block_threads", C.c_int), ("graph_steps", C.c_int),
+                ("bytes_per_step", C.c_double), ("dof_per_step", C.c_double)]
+
+
+_LIB = None
+
+
+def lib(path: str | None = None):
+    global _LIB
+    if _LIB is None:
+        so = path or _build.gpu_library()
+        L = C.CDLL(so)
+        L.dg_gpu_default_opts.argtypes = [C.c_void_p]
+        L.dg_gpu_init.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        L.dg_gpu_step.argtypes = [C.c_void_p, C.c_long]
+        L.dg_gpu_step_timed.argtypes = [C.c_void_p, C.c_long]
+        L.dg_gpu_fetch.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.dg_gpu_load.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.dg_gpu_reset.argtypes = [C.c_void_p]
+        L.dg_gpu_set_wavelet.argtypes = [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p]
+        L.dg_gpu_flush_l2.argtypes = [C.c_void_p]
+        L.dg_gpu_stats_get.argtypes = [C.c_void_p, C.c_void_p]
+        L.dg_gpu_steps_done.argtypes = [C.c_void_p]
+        L.dg_gpu_steps_done.restype = C.c_long
+        L.dg_gpu_free.argtypes = [C.c_void_p]
+        L.dg_gpu_strerror.restype = C.c_char_p
+        L.dg_gpu_strerror.argtypes = [C.c_int]
+        L.dg_gpu_last_error.restype = C.c_char_p
+        for n in ("dg_gpu_init", "dg_gpu_step", "dg_gpu_step_timed", "dg_gpu_fetch", "dg_gpu_load", "dg_gpu_reset",
+                  "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_free"):
+            getattr(L, n).restype = C.c_int
+        _LIB = L
+    return _LIB
+
+
+def _check(rc, where):
+    if rc != 0:
+        raise DGError(rc, where, lib().dg_gpu_last_error().decode(errors="replace"))
+
+
+_INTS = {"ibe", "Neighbor", "Node_Neighbor", "Edge_flag", "source", "receiver", "Triangle"}
+
+
+def mesh_from_setup(setup, *, wavelet=None, with_ref_ops: bool = True) -> dict:
+    """Collect the arrays of a host ``Setup`` (or a golden fixture) that dg_gpu_init takes."""
+    a = setup.arrays if hasattr(setup, "arrays") else setup
+    get = (lambda n: a[n]) if isinstance(a, dict) else (lambda n: getattr(a, n))
+    d = {"Point": setup.Point if hasattr(setup, "Point") else get("Point"),
+         "Triangle": setup.Triangle if hasattr(setup, "Triangle") else get("Triangle")}
+    ops = setup.ops if hasattr(setup, "ops") else get("ops")
+    d.update({"Vr": ops["Vr"], "Vs": ops["Vs"], "inverV": ops["inverV"], "V": ops["V"]})
+    for n in ("S", "ibe", "Neighbor", "Node_Neighbor", "Edge_flag", "A", "B", "absorb_fun", "source", "fun",
+              "receiver"):
+        d[n] = get(n)
+    if with_ref_ops:
+        for n in ("Dx", "Dz", "Q"):
+            try:
+                d[n] = get(n)
+            except (KeyError, AttributeError):
+                pass
+    d["wavelet"] = get("wavelet") if wavelet is None else wavelet
+    d["dt"] = float(setup.dt if hasattr(setup, "dt") else get("dt"))
+    return d
+
+
+class Engine:
+    """One device context over one or more meshes (all meshes step together)."""
+
+    def __init__(self, meshes, precision="fp64", *, device=0, reorder=True, block_threads=0, graph_steps=0,
+                 autotune=False, watchdog_every=0, tune_cache=None):
+        if isinstance(meshes, dict):
+            meshes = [meshes]
+        prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        self.precision = prec
+        self._keep = []
+        arr = (_Mesh * len(meshes))()
+        self.info = []
+        for k, m in enumerate(meshes):
+            conv = {}
+            for n, v in m.items():
+                if isinstance(v, np.ndarray):
+                    v = np.ascontiguousarray(v, dtype=np.int64 if n in _INTS else np.float64)
+                    self._keep.append(v)
+                conv[n] = v
+            K = conv["Triangle"].size // 3
+            S = conv["fun"].size // 6
+            R = conv["receiver"].size // 2
+            T = conv["wavelet"].size
+            ptr = lambda n: conv[n].ctypes.data if n in conv and conv[n] is not None else None  # noqa: E731
+            arr[k] = _Mesh(K=K, Np=6, Nfp=3, n_points=conv["Point"].size // 2, Point=ptr("Point"),
+                           Triangle=ptr("Triangle"), Vr=ptr("Vr"), Vs=ptr("Vs"), inverV=ptr("inverV"), V=ptr("V"),
+                           S=ptr("S"), ibe=ptr("ibe"), Neighbor=ptr("Neighbor"), Node_Neighbor=ptr("Node_Neighbor"),
+                           Edge_flag=ptr("Edge_flag"), A=ptr("A"), B=ptr("B"), Dx=ptr("Dx"), Dz=ptr("Dz"),
+                           Q=ptr("Q"), absorb_fun=ptr("absorb_fun"), n_shots=S, source=ptr("source"),
+                           fun=ptr("fun"), n_rec=R, receiver=ptr("receiver"), dt=float(conv["dt"]), n_steps=T,
+                           wavelet=ptr("wavelet"))
+            self.info.append({"K": K, "S": S, "R": R, "T": T})
+        opts = _Opts()
+        lib().dg_gpu_default_opts(C.byref(opts))
+        opts.precision = prec
+        opts.device = device
+        opts.reorder = 1 if reorder else 0
+        opts.block_threads = block_threads
+        opts.graph_steps = graph_steps
+        opts.autotune = 1 if autotune else 0
+        opts.watchdog_every = watchdog_every
+        opts.tune_cache = tune_cache.encode() if tune_cache else None
+        self._ctx = C.c_void_p()
+        _check(lib().dg_gpu_init(C.byref(self._ctx), arr, len(meshes), C.byref(opts)), "dg_gpu_init")
+        self._keep = []
+
+    # -- the reference's loop body ---------------------------------------------------------
+    def step(self, n: int = 1):
+        _check(lib().dg_gpu_step(self._ctx, int(n)), "dg_gpu_step")
+
+    def step_timed(self, n: int = 1):
+        _check(lib().dg_gpu_step_timed(self._ctx, int(n)), "dg_gpu_step_timed")
+        return self.stats()
+
+    @property
+    def steps_done(self) -> int:
+        return int(lib().dg_gpu_steps_done(self._ctx))
+
+    def fetch(self, what, mesh: int = 0, shot: int = 0) -> np.ndarray:
+        if isinstance(what, str):
+            what = FIELDS.get(what, {"trace_x": TRACE_X, "trace_z": TRACE_Z, "energy": ENERGY}.get(what, -99))
+        inf = self.info[mesh]
+        if what in (VX, VZ, TXX, TZZ, TXZ):
+            out = np.empty(inf["K"] * 6)
+        elif what in (TRACE_X, TRACE_Z):
+            out = np.empty((min(self.steps_done, inf["T"]), inf["R"]))
+        elif what == ENERGY:
+            out = np.empty(1)
+        else:
+            out = np.empty(1)
+        if out.size == 0:
+            return out
+        _check(lib().dg_gpu_fetch(self._ctx, what, mesh, shot, out.ctypes.data), "dg_gpu_fetch")
+        return out[0] if what == ENERGY else out
+
+    def load(self, what, values: np.ndarray, mesh: int = 0, shot: int = 0):
+        if isinstance(what, str):
+            what = FIELDS[what]
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        _check(lib().dg_gpu_load(self._ctx, what, mesh, shot, v.ctypes.data), "dg_gpu_load")
+
+    def reset(self):
+        _check(lib().dg_gpu_reset(self._ctx), "dg_gpu_reset")
+
+    def set_wavelet(self, t0: int, w: np.ndarray, mesh: int = 0):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        _check(lib().dg_gpu_set_wavelet(self._ctx, mesh, int(t0), w.size, w.ctypes.data), "dg_gpu_set_wavelet")
+
+    def flush_l2(self):
+        _check(lib().dg_gpu_flush_l2(self._ctx), "dg_gpu_flush_l2")
+
+    def stats(self) -> dict:
+        s = _Stats()
+        _check(lib().dg_gpu_stats_get(self._ctx, C.byref(s)), "dg_gpu_stats_get")
+        return {n: getattr(s, n) for n, _ in _Stats._fields_}
+
+    def close(self):
+        if getattr(self, "_ctx", None) is not None and self._ctx.value:
+            lib().dg_gpu_free(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,153 @@
+/*
+ * dg_gpu.h — C ABI of the B200 (sm_100a) engine for the DG elastic-wave time loop.
+ *
+ * Replaces the five per-step functions the reference's driver loop calls
+ * (DG_leap_Frog_OpenMP.c:418-437):
+ *   Absorb_Boundary     OpenMP_Function.c:5-6, 25-46
+ *   source_kernel       OpenMP_Function.c:8, 49-58
+ *   LU_Velocity         OpenMP_Function.c:12-15, 75-185
+ *   LU_Stress_Elastic   OpenMP_Function.c:17-20, 188-306
+ *   Record              OpenMP_Function.c:10, 61-72
+ * with one context that owns the device copies of the set-up arrays and advances any number of
+ * steps per call.  The host keeps the reference's role: it reads meshes and operator files,
+ * runs the set-up of fun_DG.c and hands the resulting arrays (exactly as fun_DG.c produces
+ * them: element-major doubles, 1-based `long` index maps) to dg_gpu_init.
+ *
+ * Conventions: every function returns DG_OK (0) or a negative DG_ERR_* code and never exits
+ * the process; a context is used from one host thread at a time and owns one CUDA stream;
+ * calls return after the device work they launched has finished unless stated otherwise.
+ */
+#ifndef DG_GPU_H
+#define DG_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DG_OK 0
+#define DG_ERR_ARG -1          /* null pointer, bad size, bad enum */
+#define DG_ERR_CUDA -2         /* a CUDA call failed (message via dg_gpu_last_error) */
+#define DG_ERR_NOMEM -3        /* device or host allocation failed */
+#define DG_ERR_MESH -4         /* index maps inconsistent (index out of range, maps not P2 faces) */
+#define DG_ERR_NONFINITE -5    /* the watchdog found NaN/Inf in the velocity fields */
+#define DG_ERR_STATE -6        /* stepping past the wavelet table, fetch of an unknown item */
+#define DG_ERR_UNSUPPORTED -7  /* Np != 6, Nfp != 3, more meshes than supported */
+#define DG_ERR_NODEVICE -8     /* no CUDA device, or not an sm_100 device */
+#define DG_ERR_ORIENTATION -9  /* a triangle with non-positive Jacobian (compact paths need CCW) */
+
+/* arithmetic of the time loop */
+#define DG_FP64_REF 0    /* the reference's per-element Dx/Dz/Q/A/B arrays, its operation order,
+                            no FMA contraction: bit-identical to OpenMP_Function.c */
+#define DG_FP64 1        /* geometric-factor form (Dr, Ds, rx..sz, LIFT): FP64 fields */
+#define DG_FP32 2        /* FP32 fields and arithmetic, factors computed in FP64 and rounded */
+#define DG_FP32_KAHAN 3  /* FP32 with a compensated (Kahan) update of every field */
+
+/* items for dg_gpu_fetch / dg_gpu_load */
+#define DG_VX 0
+#define DG_VZ 1
+#define DG_TXX 2
+#define DG_TZZ 3
+#define DG_TXZ 4
+#define DG_TRACE_X 5   /* [steps_done][n_rec] like the reference's record_x[time*Channel + k] */
+#define DG_TRACE_Z 6
+#define DG_ENERGY 7    /* one double: 1/2 sum_e J_e (rho |v|^2 + sigma:C^-1 sigma) with the P2 mass matrix */
+
+#define DG_MAX_MESHES 64
+
+typedef struct dg_gpu_ctx dg_gpu_ctx;
+
+/* One mesh with its medium, shots and receivers: the arrays of DG_leap_Frog_OpenMP.c:main
+ * after set-up (fun_DG.c producers in brackets). */
+typedef struct {
+	long K;                    /* Tri: number of triangles */
+	int Np, Nfp;               /* must be 6 and 3 (P2) */
+	long n_points;             /* Point_Num */
+	const double *Point;       /* [n_points][2]                                    (Mesh_Input) */
+	const long *Triangle;      /* [K][3] 1-based vertex ids                        (Mesh_Input) */
+	const double *Vr, *Vs;     /* [Np][Np] gradient Vandermonde (read from Vr.txt / Vs.txt) */
+	const double *inverV;      /* [Np][Np] (inverV.txt) */
+	const double *V;           /* [Np][Np] (V.txt); used for the energy mass matrix, may be NULL */
+	const double *S;           /* [3][Np][Nfp] face lift (DG_leap_Frog_OpenMP.c:306-314) */
+	const long *ibe;           /* [3][Nfp] 1-based face nodes                      (IBE) */
+	const long *Neighbor;      /* [K][3] 1-based, boundary -> 1                    (Neighbor_Edge) */
+	const long *Node_Neighbor; /* [K][3][Nfp] 1-based                              (NeighborNodes) */
+	const long *Edge_flag;     /* [K][3] 1 interior face, 0 outer boundary         (Neighbor_Edge) */
+	const double *A, *B;       /* [K][5]                                           (Elastic_A_B) */
+	const double *Dx, *Dz;     /* [K][Np][Np]  DG_FP64_REF only, else may be NULL  (Dx_Dz) */
+	const double *Q;           /* [K][3][5][2] DG_FP64_REF only, else may be NULL  (Central_flux) */
+	const double *absorb_fun;  /* [K][Np]                                          (Absorbing_Fun) */
+	int n_shots;               /* shots advanced together (the driver's m loop) */
+	const long *source;        /* [n_shots][2] (triangle, node) 1-based            (Get_Source) */
+	const double *fun;         /* [n_shots][Np] source vector (DG_leap_Frog_OpenMP.c:233-246) */
+	int n_rec;                 /* receivers, shared by all shots */
+	const long *receiver;      /* [n_rec][2] (triangle, node) 1-based, stride 2    (Get_Receiver) */
+	double dt;                 /* Calculate_Time_Step */
+	long n_steps;              /* length of wavelet[] = steps this mesh runs */
+	const double *wavelet;     /* [n_steps] Ricker_Source(t, dt, t0) */
+} dg_gpu_mesh;
+
+typedef struct {
+	int precision;       /* DG_FP64_REF / DG_FP64 / DG_FP32 / DG_FP32_KAHAN */
+	int device;          /* CUDA device ordinal */
+	int reorder;         /* 1: renumber elements along a Hilbert curve of centroids for locality */
+	int block_threads;   /* threads per block, 0: automatic (or autotuned) */
+	int graph_steps;     /* steps per captured CUDA graph, 0: automatic, <0: no graphs */
+	int autotune;        /* 1: time candidate block sizes at init */
+	int watchdog_every;  /* check the velocity fields for NaN/Inf every k steps (0: off) */
+	const char *tune_cache; /* file that keeps autotune results between runs (NULL: none) */
+} dg_gpu_opts;
+
+typedef struct {
+	double ms_velocity;  /* device time of the last timed velocity half-steps (sum) */
+	double ms_stress;    /* device time of the last timed stress half-steps (sum) */
+	long launches;       /* kernels launched by the last dg_gpu_step/dg_gpu_step_timed */
+	long steps_done;     /* steps taken so far (the `time` of the reference loop) */
+	int block_threads;   /* block size in use */
+	int graph_steps;     /* steps per graph in use */
+	double bytes_per_step; /* algorithmic HBM bytes one step of all meshes moves */
+	double dof_per_step;   /* 30 * sum over meshes of K * n_shots */
+} dg_gpu_stats;
+
+void dg_gpu_default_opts(dg_gpu_opts *opts);
+
+/* Copy the meshes to the device and prepare the kernels.  The host arrays may be freed
+ * afterwards.  State starts at zero (the per-shot memset of DG_leap_Frog_OpenMP.c:412-416). */
+int dg_gpu_init(dg_gpu_ctx **ctx, const dg_gpu_mesh *meshes, int n_meshes, const dg_gpu_opts *opts);
+
+/* Advance every mesh by n steps (meshes whose n_steps are reached stay put).
+ * Stepping past the longest wavelet table returns DG_ERR_STATE without doing anything. */
+int dg_gpu_step(dg_gpu_ctx *ctx, long n);
+
+/* Same, timing each velocity and stress half-step with CUDA events on the context stream;
+ * the sums land in dg_gpu_stats (ms_velocity, ms_stress). */
+int dg_gpu_step_timed(dg_gpu_ctx *ctx, long n);
+
+/* Copy one item of one mesh/shot to host memory `dst`, in the reference's layout:
+ * fields as double[K][Np] in the caller's element numbering, traces as double[steps][n_rec],
+ * energy as one double. */
+int dg_gpu_fetch(dg_gpu_ctx *ctx, int what, int mesh, int shot, double *dst);
+
+/* Overwrite one field of one mesh/shot from host memory (checkpoint restore); layout as fetch. */
+int dg_gpu_load(dg_gpu_ctx *ctx, int what, int mesh, int shot, const double *src);
+
+/* Zero every field and trace and rewind to step 0. */
+int dg_gpu_reset(dg_gpu_ctx *ctx);
+
+/* Replace wavelet samples [t0, t0+n) of one mesh with host values (the reference computes
+ * w(t) on the host every step, DG_leap_Frog_OpenMP.c:421). */
+int dg_gpu_set_wavelet(dg_gpu_ctx *ctx, int mesh, long t0, long n, const double *w);
+
+/* Write a buffer larger than L2 on the context stream (timing hygiene between measurements). */
+int dg_gpu_flush_l2(dg_gpu_ctx *ctx);
+
+int dg_gpu_stats_get(dg_gpu_ctx *ctx, dg_gpu_stats *out);
+long dg_gpu_steps_done(dg_gpu_ctx *ctx);
+int dg_gpu_free(dg_gpu_ctx *ctx);
+const char *dg_gpu_strerror(int code);
+/* Text of the last CUDA error seen by this thread ("" if none). */
+const char *dg_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

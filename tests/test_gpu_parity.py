@@ -1,0 +1,234 @@
+"""GPU engine against the reference (golden fixtures) and the CPU oracle, through the C ABI.
+
+Tolerances (relative L2 over all samples):
+  DG_FP64_REF   bit-identical to the reference's OpenMP code (values compared with ==)
+  DG_FP64       <= 1e-10   (geometric-factor form, FMA)
+  DG_FP32       <= 1e-4    trace error against FP64
+  DG_FP32_KAHAN <= 1e-4    and no worse than plain FP32 on the final fields
+"""
+import numpy as np
+import pytest
+
+from conftest import Golden, golden_names, pkg, rel_l2
+
+import oracle
+
+eng = pkg.engine
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("Vx", "Vz", "Txx", "Tzz", "Txz")
+
+
+def _engine(g: Golden, precision, **kw):
+    a = g.setup_arrays()
+    return eng.Engine(eng.mesh_from_setup(a), precision, **kw)
+
+
+def _run_and_collect(e: eng.Engine, g: Golden, shot: int):
+    snaps = {}
+    for t0 in range(0, g.steps, g.snap_every):
+        e.step(g.snap_every)
+        t1 = t0 + g.snap_every
+        snaps[t1] = (e.fetch("Vx", 0, shot), e.fetch("Vz", 0, shot))
+    return snaps
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fp64_ref_bit_identical_to_reference(name):
+    g = Golden(name)
+    with _engine(g, "fp64_ref") as e:
+        for t0 in range(0, g.steps, g.snap_every):
+            e.step(g.snap_every)
+            t1 = t0 + g.snap_every
+            for m in range(g.shots):
+                assert np.array_equal(e.fetch("Vx", 0, m), g.z["shot%d_Vx%d" % (m, t1)]), (m, t1)
+                assert np.array_equal(e.fetch("Vz", 0, m), g.z["shot%d_Vz%d" % (m, t1)]), (m, t1)
+        for m in range(g.shots):
+            assert np.array_equal(e.fetch("trace_x", 0, m), g.z["shot%d_rec_x" % m])
+            assert np.array_equal(e.fetch("trace_z", 0, m), g.z["shot%d_rec_z" % m])
+            for f in FIELDS:
+                assert np.array_equal(e.fetch(f, 0, m), g.z["shot%d_final_%s" % (m, f)]), f
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 1e-4), ("fp32_kahan", 1e-4)])
+def test_compact_paths_against_reference(name, precision, tol):
+    g = Golden(name)
+    with _engine(g, precision) as e:
+        e.step(g.steps)
+        for m in range(g.shots):
+            tx = e.fetch("trace_x", 0, m)
+            tz = e.fetch("trace_z", 0, m)
+            err = rel_l2(np.concatenate([tx, tz]), np.concatenate([g.z["shot%d_rec_x" % m], g.z["shot%d_rec_z" % m]]))
+            assert err <= tol, (precision, m, err)
+            for f in FIELDS:
+                assert rel_l2(e.fetch(f, 0, m), g.z["shot%d_final_%s" % (m, f)]) <= 10 * tol, f
+
+
+def test_kahan_not_worse_than_fp32():
+    g = Golden("square_K288")
+    errs = {}
+    for p in ("fp32", "fp32_kahan"):
+        with _engine(g, p) as e:
+            e.step(g.steps)
+            errs[p] = sum(rel_l2(e.fetch(f), g.z["shot0_final_%s" % f]) for f in FIELDS)
+    assert errs["fp32_kahan"] <= errs["fp32"] * 1.05, errs
+
+
+@pytest.mark.parametrize("precision", ["fp64_ref", "fp64", "fp32"])
+def test_reordering_does_not_change_results(precision):
+    g = Golden("slope_coupled")
+    out = []
+    for reorder in (False, True):
+        with _engine(g, precision, reorder=reorder) as e:
+            e.step(g.steps)
+            out.append([e.fetch(f) for f in FIELDS] + [e.fetch("trace_x")])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
+def test_block_sizes_and_graphs_agree():
+    g = Golden("square_3shots")
+    ref = None
+    for block, graph in ((64, -1), (128, 7), (256, 0)):
+        with _engine(g, "fp64", block_threads=block, graph_steps=graph) as e:
+            e.step(g.steps)
+            got = [e.fetch(f, 0, m) for m in range(g.shots) for f in FIELDS]
+        if ref is None:
+            ref = got
+        else:
+            for a, b in zip(ref, got):
+                assert np.array_equal(a, b)
+
+
+def test_multi_mesh_batch_matches_single_runs():
+    gs = [Golden(n) for n in golden_names()]
+    meshes = [eng.mesh_from_setup(g.setup_arrays()) for g in gs]
+    with eng.Engine(meshes, "fp64") as e:
+        e.step(max(g.steps for g in gs))
+        batch = [[e.fetch(f, k, m) for m in range(g.shots) for f in FIELDS] for k, g in enumerate(gs)]
+        traces = [[e.fetch("trace_x", k, m) for m in range(g.shots)] for k, g in enumerate(gs)]
+    for k, g in enumerate(gs):
+        with _engine(g, "fp64") as e:
+            e.step(g.steps)
+            single = [e.fetch(f, 0, m) for m in range(g.shots) for f in FIELDS]
+            for m in range(g.shots):
+                assert np.array_equal(traces[k][m], e.fetch("trace_x", 0, m))
+        for a, b in zip(batch[k], single):
+            assert np.array_equal(a, b)
+
+
+def test_checkpoint_restore_continues_identically():
+    """Fields fetched at step 80 and loaded into a second context continue bit-identically."""
+    g = Golden("square_K288")
+    with _engine(g, "fp64_ref") as a, _engine(g, "fp64_ref") as b:
+        a.step(80)
+        state = [a.fetch(f) for f in FIELDS]
+        a.step(g.steps - 80)
+        final = [a.fetch(f) for f in FIELDS]
+        # b runs its first 80 steps without a source (state stays zero), then takes the checkpoint
+        b.set_wavelet(0, np.zeros(80))
+        b.step(80)
+        assert not np.any(b.fetch("Vz"))
+        for f, v in zip(FIELDS, state):
+            b.load(f, v)
+        b.step(g.steps - 80)
+        for x, y in zip(final, [b.fetch(f) for f in FIELDS]):
+            assert np.array_equal(x, y)
+        b.reset()
+        assert b.steps_done == 0 and not np.any(b.fetch("Vx"))
+
+
+def test_host_wavelet_update_equals_table():
+    g = Golden("square_K288")
+    a = g.setup_arrays()
+    with _engine(g, "fp64") as e1, _engine(g, "fp64") as e2:
+        e1.step(g.steps)
+        for t0 in range(0, g.steps, 50):
+            e2.set_wavelet(t0, a["wavelet"][t0:t0 + 50])
+            e2.step(50)
+        assert np.array_equal(e1.fetch("trace_z"), e2.fetch("trace_z"))
+
+
+def test_linearity_power_of_two_bit_exact():
+    """Doubling the source doubles every value exactly, in every arithmetic."""
+    g = Golden("slope_coupled")
+    a = g.setup_arrays()
+    for p in ("fp64", "fp32"):
+        m1 = eng.mesh_from_setup(a)
+        m2 = eng.mesh_from_setup(a, wavelet=2.0 * a["wavelet"])
+        with eng.Engine(m1, p) as e1, eng.Engine(m2, p) as e2:
+            e1.step(g.steps)
+            e2.step(g.steps)
+            assert np.array_equal(2.0 * e1.fetch("trace_x"), e2.fetch("trace_x"))
+            assert np.array_equal(2.0 * e1.fetch("Txz"), e2.fetch("Txz"))
+
+
+def test_energy_fp32_tracks_fp64():
+    g = Golden("slope_coupled")
+    en = {}
+    for p in ("fp64", "fp32", "fp32_kahan"):
+        with _engine(g, p) as e:
+            vals = []
+            for _ in range(g.steps // 25):
+                e.step(25)
+                vals.append(e.fetch("energy"))
+            en[p] = np.array(vals)
+    assert np.all(en["fp64"] >= 0) and en["fp64"].max() > 0
+    for p in ("fp32", "fp32_kahan"):
+        drift = np.max(np.abs(en[p] - en["fp64"])) / en["fp64"].max()
+        assert drift < 1e-4, (p, drift)
+
+
+def test_errors_are_reported_not_raised_on_device():
+    g = Golden("square_K288")
+    with _engine(g, "fp64", watchdog_every=10) as e:
+        with pytest.raises(eng.DGError) as ei:
+            e.step(g.steps + 1)
+        assert ei.value.code == -6  # DG_ERR_STATE: past the wavelet table, nothing ran
+        assert e.steps_done == 0
+        e.step(10)
+        bad = e.fetch("Vx")
+        bad[7] = np.nan
+        e.load("Vx", bad)
+        with pytest.raises(eng.DGError) as ei:
+            e.step(10)
+        assert ei.value.code == -5  # DG_ERR_NONFINITE from the watchdog
+
+
+def test_invalid_maps_rejected_on_host():
+    g = Golden("square_K288")
+    a = g.setup_arrays()
+    m = eng.mesh_from_setup(a)
+    m["Neighbor"] = m["Neighbor"].copy()
+    m["Neighbor"].ravel()[5] = 10 ** 6
+    with pytest.raises(eng.DGError) as ei:
+        eng.Engine(m, "fp64")
+    assert ei.value.code == -4
+    m = eng.mesh_from_setup(a)
+    t = m["Triangle"].copy().reshape(-1, 3)
+    t[3, [1, 2]] = t[3, [2, 1]]
+    m["Triangle"] = t
+    with pytest.raises(eng.DGError) as ei:
+        eng.Engine(m, "fp64")
+    assert ei.value.code == -9
+
+
+@pytest.mark.slow
+def test_homogeneous_square_full_size_against_oracle():
+    """The 20,000-element square, 400 steps: FP64 within 1e-10 of the oracle, REF bit-exact."""
+    w = pkg.workloads.homogeneous_square(steps=400)
+    s = pkg.host.build_setup(w)
+    o = oracle.Oracle.from_setup(s)
+    rx, rz = o.run(0, w.steps, threads=0)
+    ref_fields = [f.copy() for f in o.fields]
+    for p, tol in (("fp64_ref", 0.0), ("fp64", 1e-10), ("fp32", 1e-4)):
+        with eng.Engine(eng.mesh_from_setup(s), p) as e:
+            e.step(w.steps)
+            tx, tz = e.fetch("trace_x"), e.fetch("trace_z")
+            if tol == 0.0:
+                assert np.array_equal(tx, rx) and np.array_equal(tz, rz)
+                for k, f in enumerate(FIELDS):
+                    assert np.array_equal(e.fetch(f), ref_fields[k])
+            else:
+                assert rel_l2(np.concatenate([tx, tz]), np.concatenate([rx, rz])) <= tol

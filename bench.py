@@ -1,0 +1,382 @@
+#!/usr/bin/env python3
+"""Benchmark of the DG elastic-wave time loop on B200.
+
+One bench step = one time step of the whole workload: sponge, source, velocity half-step,
+stress half-step and receiver record for every element and shot.  The default workload is the
+multi-shot batch: a layered elastic mesh of 200,000 triangles advanced for 64 shots at once in
+FP32 (shots innermost).  Beside it the line reports the plain FP64 path (one shot, L2 flushed
+between steps), the FP32-vs-FP64 trace error, the roofline of the dominant kernel, an
+end-to-end figure through the public API with host buffers, and the reference's own CPU code
+timed on this host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Under torchrun (N > 1) every rank advances its own 64-shot batch (shots shifted along the
+surface per rank, no collective on the data path); the time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF-updates/s batched FP32 vs plain FP64 at ≤1e-4 trace L2; HBM % of peak"
+UNIT = "DOF-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def pkg():
+    return importlib.import_module("discontinuous-galerkin-method_b200")
+
+
+WORKLOADS = {
+    # name: (constructor(steps, rank), description)
+    "multishot": (lambda steps, rank: pkg().workloads.layered_multishot(steps=steps, shot_phase=(rank % 16) / 16.0),
+                  "multi-shot layered elastic batch: 200,000 triangles x 64 shots"),
+    "slope": (lambda steps, rank: pkg().workloads.coupled_slope(steps=steps),
+              "coupled acoustic-elastic slope: ~400,000 triangles, 1 shot"),
+    "random": (lambda steps, rank: pkg().workloads.random_medium(steps=steps),
+               "heterogeneous random medium: 2,000,000 triangles, 1 shot"),
+    "square": (lambda steps, rank: pkg().workloads.homogeneous_square(steps=steps),
+               "homogeneous square: 20,000 triangles, 1 shot"),
+}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the GPU works."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = os.environ.get("DG_BENCH_BACKEND", "nccl")
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return rank, world, local, dist
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device):
+    if dist is not None:
+        import torch
+        dist.barrier()
+        torch.cuda.synchronize(device)
+
+
+def cpu_reference(w, steps_hint: float = 12.0, force_port: bool = False):
+    """Time the reference's own OpenMP code (oracle/_ref) on this host: one shot, all cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun  # CPU-baseline leg only
+
+    cores = os.cpu_count() or 1
+    w1 = pkg().workloads.Workload(w.name, w.mesh, w.vp, w.vs, w.rho, w.fp, w.sponge, w.src[:1], w.rec, w.steps)
+    if refrun.available(w1) and not force_port:
+        with tempfile.TemporaryDirectory() as d:
+            probe = refrun.run(w1, os.path.join(d, "p"), steps=5, threads=cores, dump_setup=0, work_dir=os.path.join(d, "w"))
+            per = probe["timing"]["loop_seconds"] / 5
+            n = int(max(10, min(w.steps, steps_hint / max(per, 1e-6))))
+            r = refrun.run(w1, os.path.join(d, "r"), steps=n, threads=cores, dump_setup=0, work_dir=os.path.join(d, "w"))
+            sec = r["timing"]["loop_seconds"]
+            th = int(r["timing"]["threads"])
+        kind = "reference"
+    else:
+        import oracle
+        s = pkg().host.build_setup(w1, full=True, n_steps=max(w.steps, 10))
+        o = oracle.Oracle.from_setup(s)
+        t = time.perf_counter()
+        o.run(0, 3, threads=cores, record=True)
+        per = (time.perf_counter() - t) / 3
+        n = int(max(10, min(s.n_steps - 3, steps_hint / max(per, 1e-6))))
+        t = time.perf_counter()
+        o.run(0, n, threads=cores, record=True)
+        sec = time.perf_counter() - t
+        th = cores
+        kind = "port"
+    dof = 30.0 * w1.K * n
+    return {"value": dof / sec, "unit": UNIT, "cores": th, "kind": kind,
+            "sample": "1 of %d shots, first %d time steps, K=%d, OpenMP %d threads, loop time only (%.1f s)"
+                      % (w.shots, n, w1.K, th, sec)}
+
+
+def run_reference_arm(args):
+    rank, world, local, dist = dist_setup(args)
+    if rank != 0:
+        return 0
+    ctor, desc = WORKLOADS[args.workload]
+    w = ctor(max(args.steps, args.warmup) + 10, 0)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+    cores = os.cpu_count() or 1
+    w1 = pkg().workloads.Workload(w.name, w.mesh, w.vp, w.vs, w.rho, w.fp, w.sponge, w.src[:1], w.rec, w.steps)
+    with tempfile.TemporaryDirectory() as d:
+        if refrun.available(w1):
+            if args.warmup:
+                refrun.run(w1, os.path.join(d, "w"), steps=args.warmup, threads=cores, dump_setup=0,
+                           work_dir=os.path.join(d, "in"))
+            r = refrun.run(w1, os.path.join(d, "t"), steps=args.steps, threads=cores, dump_setup=0,
+                           work_dir=os.path.join(d, "in"))
+            sec = r["timing"]["loop_seconds"]
+            kind, th = "reference", int(r["timing"]["threads"])
+        else:
+            import oracle
+            s = pkg().host.build_setup(w1, full=True)
+            o = oracle.Oracle.from_setup(s)
+            o.run(0, args.warmup, threads=cores)
+            t = time.perf_counter()
+            o.run(0, args.steps, threads=cores)
+            sec = time.perf_counter() - t
+            kind, th = "port", cores
+    value = 30.0 * w1.K * args.steps / sec
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "shots_timed": 1, "K": w1.K, "threads": th},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": kind,
+                             "sample": "1 shot, %d time steps after %d warm-up steps" % (args.steps, args.warmup)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def read_traffic(workload: str, kernel: str):
+    """DRAM bytes per launch from the committed ncu summary (profiles/), if one exists."""
+    p = os.path.join(ROOT, "profiles", "traffic_%s_%s.txt" % (kernel, workload))
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    rank, world, local, dist = dist_setup(args)
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the engine has no CPU fallback)")
+    device = local
+    torch.cuda.set_device(device)
+    P = pkg()
+    eng = P.engine
+    ctor, desc = WORKLOADS[args.workload]
+    K_steps, W_steps = args.steps, args.warmup
+    e2e_chunk = 25
+    e2e_steps = max(e2e_chunk, (K_steps // e2e_chunk) * e2e_chunk)
+    acc_steps = 200
+    table = max(W_steps + K_steps, W_steps + e2e_steps, acc_steps) + 8
+    w = ctor(table, rank)
+    s = P.host.build_setup(w, full=False, n_steps=table)
+    mesh = eng.mesh_from_setup(s, with_ref_ops=False)
+    peak, peak_src = peaks()
+    sampler = ClockSampler(device)
+    sampler.start()
+
+    # ---- headline: batched FP32, inputs resident in HBM ------------------------------------
+    e = eng.Engine(mesh, "fp32", device=device)
+    st = e.stats()
+    bytes_step = st["bytes_per_step"]
+    dof_step = st["dof_per_step"]
+    e.step(W_steps)
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    mv, ms, total_ms = e.step_profiled(K_steps)
+    torch.cuda.synchronize(device)
+    barrier(dist, device)
+    t_max = max_over_ranks(total_ms, dist, device)
+    value = world * dof_step * K_steps / (t_max * 1e-3)
+
+    # per-kernel roofline (algorithmic bytes per launch / mean launch time)
+    S, Kel, wsz = w.shots, w.K, 4
+    b_vel = Kel * (42 * S * wsz + 5 * wsz + 16)
+    b_str = Kel * (48 * S * wsz + 8 * wsz + 16)
+    t_vel, t_str = float(np.mean(mv)), float(np.mean(ms))
+    dom = ("k_stress", b_str, t_str) if t_str >= t_vel else ("k_velocity", b_vel, t_vel)
+    achieved = dom[1] / (dom[2] * 1e-3) / 1e9
+    traffic = read_traffic(args.workload, dom[0])
+
+    # ---- end to end through the public API with pinned host buffers ------------------------
+    e.reset()
+    e.step(W_steps)
+    R = w.rec.shape[0]
+    wav = torch.empty(e2e_chunk, dtype=torch.float64).pin_memory()
+    wav.copy_(torch.from_numpy(np.ascontiguousarray(s.arrays["wavelet"][:e2e_chunk])))
+    out_x = torch.empty((S, e2e_chunk, R), dtype=torch.float64).pin_memory()
+    out_z = torch.empty((S, e2e_chunk, R), dtype=torch.float64).pin_memory()
+    barrier(dist, device)
+    t0 = time.perf_counter()
+    for c in range(e2e_steps // e2e_chunk):
+        t_at = W_steps + c * e2e_chunk
+        wav.copy_(torch.from_numpy(s.arrays["wavelet"][t_at:t_at + e2e_chunk]))
+        e.set_wavelet(t_at, wav)
+        e.step(e2e_chunk)
+        e.fetch_traces(t_at, e2e_chunk, out_x=out_x, out_z=out_z)
+    t_e2e = time.perf_counter() - t0
+    barrier(dist, device)
+    t_e2e = max_over_ranks(t_e2e, dist, device)
+    e2e_value = world * dof_step * e2e_steps / t_e2e
+    h2d = 8.0  # one wavelet sample per step
+    d2h = 2.0 * S * R * 8.0
+
+    # ---- accuracy: FP32 batch against FP64 batch over the first steps -----------------------
+    e.reset()
+    e.step(acc_steps)
+    tr32 = [e.fetch("trace_x", 0, m) for m in range(S)] + [e.fetch("trace_z", 0, m) for m in range(S)]
+    e.close()
+    with eng.Engine(mesh, "fp64", device=device) as e64:
+        e64.step(acc_steps)
+        tr64 = [e64.fetch("trace_x", 0, m) for m in range(S)] + [e64.fetch("trace_z", 0, m) for m in range(S)]
+    a32, a64 = np.concatenate([x.ravel() for x in tr32]), np.concatenate([x.ravel() for x in tr64])
+    trace_err = float(np.linalg.norm(a32 - a64) / max(np.linalg.norm(a64), 1e-300))
+
+    # ---- plain FP64 path on the same mesh: one shot, L2 flushed before every step -----------
+    w1 = P.workloads.Workload(w.name, w.mesh, w.vp, w.vs, w.rho, w.fp, w.sponge, w.src[:1], w.rec, w.steps)
+    s1 = P.host.build_setup(w1, full=False, n_steps=table)
+    with eng.Engine(eng.mesh_from_setup(s1, with_ref_ops=False), "fp64", device=device) as e1:
+        e1.step(W_steps)
+        mv1, ms1, tot1 = e1.step_profiled(K_steps, flush_l2=True)
+        fp64_value = e1.stats()["dof_per_step"] * K_steps / (tot1 * 1e-3)
+        fp64_bytes = e1.stats()["bytes_per_step"]
+    clocks = sampler.stop()
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K_steps, "warmup": W_steps,
+            "ms_per_step": t_max / K_steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded jittered-grid mesh, layered medium)",
+            "config": {"workload": desc, "K": Kel, "shots": S, "receivers": R, "precision": "fp32",
+                       "parallelism": "independent shot batches per GPU" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2: state %.2f GB per GPU" % (30 * S * Kel * 4 / 1e9),
+                       "block_threads": st["block_threads"]},
+            "gpu_launches": 2 * K_steps,
+            "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                         "bytes_per_launch": dom[1], "ms_per_launch": dom[2],
+                         "step_GBs": bytes_step / (t_max / K_steps * 1e-3) / 1e9,
+                         "kernels": {"k_velocity": {"ms": t_vel, "GBs": b_vel / (t_vel * 1e-3) / 1e9},
+                                     "k_stress": {"ms": t_str, "GBs": b_str / (t_str * 1e-3) / 1e9}}},
+            "fp64_plain": {"value": fp64_value, "unit": UNIT, "shots": 1, "l2": "flushed before every step",
+                           "ms_per_step": tot1 / K_steps,
+                           "GBs": fp64_bytes / (tot1 / K_steps * 1e-3) / 1e9,
+                           "ratio_fp32_batched_over_fp64_plain": value / world / fp64_value},
+            "accuracy": {"trace_rel_l2_fp32_vs_fp64": trace_err, "steps": acc_steps, "shots": S},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "chunk_steps": e2e_chunk,
+                    "what": "dg_gpu_set_wavelet (pinned host wavelet) + dg_gpu_step + dg_gpu_fetch_traces "
+                            "(all shots, pinned host buffers) per %d-step chunk, wall clock" % e2e_chunk},
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference(w)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="multishot")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

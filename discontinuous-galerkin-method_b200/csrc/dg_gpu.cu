@@ -656,9 +656,10 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
       if ((rc = upload_mesh<float>(c.get(), meshes[k], p, c->md_f.back()))) return rc;
     }
     c->max_steps = std::max(c->max_steps, h.steps);
-    // algorithmic bytes per step: 90 state values (+60 compensation values) per element and shot,
-    // plus per element geo + mat (2 x 4 values) and face codes (2 x 16 B) over the two half-steps
-    double per = 90.0 * h.S * w + (c->kahan ? 60.0 * h.S * 4 : 0.0) + 16.0 * w + 32.0;
+    // algorithmic bytes per step: 90 state values (+60 compensation values) per element and shot
+    // (velocity pass reads 30 and writes 12, stress pass reads 30 and writes 18), plus per element
+    // geo (2 x 4 values), 1/rho (1 value), lambda/mu/lambda+2mu (4 values) and face codes (2 x 16 B)
+    double per = 90.0 * h.S * w + (c->kahan ? 60.0 * h.S * 4 : 0.0) + 13.0 * w + 32.0;
     if (o.precision == DG_FP64_REF) per = 90.0 * h.S * 8 + 2.0 * 72 * 8 + 30 * 8 + 10 * 8 + 32.0;
     bytes += per * (double)h.K;
     dof += 30.0 * (double)h.K * h.S;
@@ -747,6 +748,89 @@ static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
 int dg_gpu_step(dg_gpu_ctx* c, long n) { return do_steps(c, n, false); }
 int dg_gpu_step_timed(dg_gpu_ctx* c, long n) { return do_steps(c, n, true); }
 
+static int ensure_flush(dg_gpu_ctx* c) {
+  if (c->d_flush) return DG_OK;
+  c->flush_bytes = (size_t)256 << 20;  // twice the 126 MB L2
+  void* p = nullptr;
+  CK(cudaMalloc(&p, c->flush_bytes));
+  c->allocs.push_back(p);
+  c->d_flush = p;
+  return DG_OK;
+}
+
+static int ensure_stage(dg_gpu_ctx* c, size_t elems) {
+  if (elems <= c->stage_elems) return DG_OK;
+  double* p = nullptr;
+  int rc = c->alloc(&p, elems);
+  if (rc) return rc;
+  c->d_stage = p;
+  c->stage_elems = elems;
+  return DG_OK;
+}
+
+int dg_gpu_step_profiled(dg_gpu_ctx* c, long n, int flush_l2, float* ms_vel, float* ms_str, double* ms_total) {
+  if (!c || n < 0) return fail(DG_ERR_ARG, "bad arguments");
+  if (c->t + n > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
+  CK(cudaSetDevice(c->device));
+  int rc;
+  if (flush_l2 && (rc = ensure_flush(c))) return rc;
+  std::vector<cudaEvent_t> ev((size_t)3 * n);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  for (long k = 0; k < n; k++) {
+    if (flush_l2) CK(cudaMemsetAsync(c->d_flush, (int)(k & 0xff), c->flush_bytes, c->stream));
+    if ((rc = launch_step(c, ev[3 * k], ev[3 * k + 1], ev[3 * k + 2]))) return rc;
+  }
+  if (n > 0) CK(cudaEventSynchronize(ev[3 * n - 1]));
+  double total = 0, sv = 0, ss = 0;
+  for (long k = 0; k < n; k++) {
+    float a = 0, b = 0;
+    CK(cudaEventElapsedTime(&a, ev[3 * k], ev[3 * k + 1]));
+    CK(cudaEventElapsedTime(&b, ev[3 * k + 1], ev[3 * k + 2]));
+    if (ms_vel) ms_vel[k] = a;
+    if (ms_str) ms_str[k] = b;
+    sv += a;
+    ss += b;
+  }
+  if (n > 0 && !flush_l2) {
+    float all = 0;
+    CK(cudaEventElapsedTime(&all, ev[0], ev[3 * n - 1]));
+    total = all;
+  } else {
+    total = sv + ss;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (ms_total) *ms_total = total;
+  c->t += n;
+  c->stats.ms_velocity = sv;
+  c->stats.ms_stress = ss;
+  c->stats.launches = 2 * n;
+  c->stats.steps_done = c->t;
+  return DG_OK;
+}
+
+int dg_gpu_fetch_traces(dg_gpu_ctx* c, int mesh, long t0, long n, double* dst_x, double* dst_z) {
+  if (!c || !dst_x || !dst_z || mesh < 0 || mesh >= (int)c->mi.size() || t0 < 0 || n < 0)
+    return fail(DG_ERR_ARG, "bad arguments");
+  const MeshHostInfo& h = c->mi[mesh];
+  if (t0 + n > std::min(c->t, h.steps)) return fail(DG_ERR_STATE, "trace window beyond the steps taken");
+  const long long per = (long long)n * h.n_rec * h.S;
+  if (per == 0) return DG_OK;
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_stage(c, (size_t)2 * per);
+  if (rc) return rc;
+  const int B = 256;
+  const int grid = (int)((2 * per + B - 1) / B);
+  if (c->is_double)
+    k_fetch_traces<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].trace, h.n_rec, h.S, t0, n, c->d_stage);
+  else
+    k_fetch_traces<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].trace, h.n_rec, h.S, t0, n, c->d_stage);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(dst_x, c->d_stage, per * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(dst_z, c->d_stage + per, per * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
 int dg_gpu_fetch(dg_gpu_ctx* c, int what, int mesh, int shot, double* dst) {
   if (!c || !dst || mesh < 0 || mesh >= (int)c->mi.size()) return fail(DG_ERR_ARG, "bad arguments");
   const MeshHostInfo& h = c->mi[mesh];
@@ -830,13 +914,8 @@ int dg_gpu_set_wavelet(dg_gpu_ctx* c, int mesh, long t0, long n, const double* w
 int dg_gpu_flush_l2(dg_gpu_ctx* c) {
   if (!c) return fail(DG_ERR_ARG, "null context");
   CK(cudaSetDevice(c->device));
-  if (!c->d_flush) {
-    c->flush_bytes = (size_t)256 << 20;
-    void* p = nullptr;
-    CK(cudaMalloc(&p, c->flush_bytes));
-    c->allocs.push_back(p);
-    c->d_flush = p;
-  }
+  int rc = ensure_flush(c);
+  if (rc) return rc;
   CK(cudaMemsetAsync(c->d_flush, (int)(c->t & 0xff), c->flush_bytes, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return DG_OK;

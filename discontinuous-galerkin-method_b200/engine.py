@@ -23,7 +23,17 @@ ERRORS = {0: "DG_OK", -1: "DG_ERR_ARG", -2: "DG_ERR_CUDA", -3: "DG_ERR_NOMEM", -
           -9: "DG_ERR_ORIENTATION"}
 
 # exported symbols of include/dg_gpu.h (checked by the CPU tests)
-EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_timed", "dg_gpu_fetch", "dg_gpu_load",
+def _ptr(a):
+    """Address of a host buffer: a numpy array or anything with data_ptr() (e.g. pinned memory)."""
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    if not a.flags["C_CONTIGUOUS"] or a.dtype != np.float64:
+        raise ValueError("need a C-contiguous float64 buffer")
+    return a.ctypes.data
+
+
+EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_timed", "dg_gpu_step_profiled",
+           "dg_gpu_fetch_traces", "dg_gpu_fetch", "dg_gpu_load",
            "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_steps_done",
            "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error"]
 
@@ -69,6 +79,10 @@ def lib(path: str | None = None):
         L.dg_gpu_init.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         L.dg_gpu_step.argtypes = [C.c_void_p, C.c_long]
         L.dg_gpu_step_timed.argtypes = [C.c_void_p, C.c_long]
+        L.dg_gpu_step_profiled.argtypes = [C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dg_gpu_step_profiled.restype = C.c_int
+        L.dg_gpu_fetch_traces.argtypes = [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
+        L.dg_gpu_fetch_traces.restype = C.c_int
         L.dg_gpu_fetch.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.dg_gpu_load.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.dg_gpu_reset.argtypes = [C.c_void_p]
@@ -172,6 +186,24 @@ class Engine:
         _check(lib().dg_gpu_step_timed(self._ctx, int(n)), "dg_gpu_step_timed")
         return self.stats()
 
+    def step_profiled(self, n: int, flush_l2: bool = False):
+        """n steps with CUDA events around every launch; returns (ms_vel[n], ms_str[n], ms_total)."""
+        mv = np.zeros(max(int(n), 1), dtype=np.float32)
+        ms = np.zeros(max(int(n), 1), dtype=np.float32)
+        tot = C.c_double(0.0)
+        _check(lib().dg_gpu_step_profiled(self._ctx, int(n), 1 if flush_l2 else 0, mv.ctypes.data, ms.ctypes.data,
+                                          C.byref(tot)), "dg_gpu_step_profiled")
+        return mv[:n], ms[:n], tot.value
+
+    def fetch_traces(self, t0: int, n: int, mesh: int = 0, out_x=None, out_z=None):
+        """Traces of steps [t0, t0+n) of all shots, shape (shots, n, n_rec) each."""
+        inf = self.info[mesh]
+        shape = (inf["S"], int(n), inf["R"])
+        ox = np.empty(shape) if out_x is None else out_x
+        oz = np.empty(shape) if out_z is None else out_z
+        _check(lib().dg_gpu_fetch_traces(self._ctx, mesh, int(t0), int(n), _ptr(ox), _ptr(oz)), "dg_gpu_fetch_traces")
+        return ox, oz
+
     @property
     def steps_done(self) -> int:
         return int(lib().dg_gpu_steps_done(self._ctx))
@@ -202,9 +234,11 @@ class Engine:
     def reset(self):
         _check(lib().dg_gpu_reset(self._ctx), "dg_gpu_reset")
 
-    def set_wavelet(self, t0: int, w: np.ndarray, mesh: int = 0):
-        w = np.ascontiguousarray(w, dtype=np.float64)
-        _check(lib().dg_gpu_set_wavelet(self._ctx, mesh, int(t0), w.size, w.ctypes.data), "dg_gpu_set_wavelet")
+    def set_wavelet(self, t0: int, w, mesh: int = 0):
+        if not hasattr(w, "data_ptr"):
+            w = np.ascontiguousarray(w, dtype=np.float64)
+        n = w.numel() if hasattr(w, "numel") else w.size
+        _check(lib().dg_gpu_set_wavelet(self._ctx, mesh, int(t0), n, _ptr(w)), "dg_gpu_set_wavelet")
 
     def flush_l2(self):
         _check(lib().dg_gpu_flush_l2(self._ctx), "dg_gpu_flush_l2")

@@ -135,11 +135,15 @@ def random_medium(width=10000.0, height=5000.0, n_cells_x=1000, n_cells_z=1000, 
                     meshgen.snap_to_vertices(mesh, rec), steps)
 
 
-def layered_multishot(nx=400, nz=250, h=20.0, shots=64, steps=4000, seed=3, n_rec=201) -> Workload:
-    """Layered elastic mesh (K = 2 nx nz), ``shots`` sources evenly spaced 200 m below the top."""
+def layered_multishot(nx=400, nz=250, h=20.0, shots=64, steps=4000, seed=3, n_rec=201,
+                      shot_phase: float = 0.0) -> Workload:
+    """Layered elastic mesh (K = 2 nx nz), ``shots`` sources evenly spaced 200 m below the top.
+
+    ``shot_phase`` in [0, 1) shifts every source along the surface by that fraction of the
+    shot spacing (a different shot set on the same mesh)."""
     width, height = nx * h, nz * h
     zsrc = height - 200.0
-    xs = [round(width * (i + 0.5) / shots / h) * h for i in range(shots)]
+    xs = [round(width * (i + 0.5 + shot_phase) / shots / h) * h for i in range(shots)]
     srcs = [(x, zsrc) for x in xs]
     mesh = meshgen.jittered_grid(nx, nz, width, height, jitter=0.1, seed=seed, pinned=srcs)
     cz = mesh.centroids()[:, 1]

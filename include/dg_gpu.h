@@ -122,6 +122,17 @@ int dg_gpu_step(dg_gpu_ctx *ctx, long n);
  * the sums land in dg_gpu_stats (ms_velocity, ms_stress). */
 int dg_gpu_step_timed(dg_gpu_ctx *ctx, long n);
 
+/* Advance n steps with a CUDA event before, between and after the two launches of every step,
+ * all on the context stream and without host synchronisation until the end.  ms_vel / ms_str
+ * (n floats each, may be NULL) receive each launch's device time; ms_total the time from the
+ * first event to the last.  With flush_l2 != 0 a buffer larger than L2 is written before every
+ * step, outside the timed launches (ms_total then counts launches only). */
+int dg_gpu_step_profiled(dg_gpu_ctx *ctx, long n, int flush_l2, float *ms_vel, float *ms_str, double *ms_total);
+
+/* Receiver traces of steps [t0, t0+n) for every shot of one mesh:
+ * dst_x / dst_z = double[n_shots][n][n_rec] (each shot like the reference's record_x window). */
+int dg_gpu_fetch_traces(dg_gpu_ctx *ctx, int mesh, long t0, long n, double *dst_x, double *dst_z);
+
 /* Copy one item of one mesh/shot to host memory `dst`, in the reference's layout:
  * fields as double[K][Np] in the caller's element numbering, traces as double[steps][n_rec],
  * energy as one double. */

@@ -134,6 +134,7 @@ def dist_setup(args):
 
 
 def max_over_ranks(x: float, dist, device) -> float:
+    """Maximum of a per-rank time over all ranks (device: a CUDA ordinal, or "cpu" for gloo)."""
     if dist is None:
         return x
     import torch
@@ -142,11 +143,18 @@ def max_over_ranks(x: float, dist, device) -> float:
     return float(t.item())
 
 
+def weak_scaling_value(dof_per_step_per_rank: float, steps: int, local_ms: float, world: int, dist, device) -> float:
+    """Whole-job DOF-updates/s: every rank's work over the slowest rank's device time."""
+    t_max = max_over_ranks(local_ms, dist, device)
+    return world * dof_per_step_per_rank * steps / (t_max * 1e-3), t_max
+
+
 def barrier(dist, device):
     if dist is not None:
         import torch
         dist.barrier()
-        torch.cuda.synchronize(device)
+        if device != "cpu":
+            torch.cuda.synchronize(device)
 
 
 def cpu_reference(w, steps_hint: float = 12.0, force_port: bool = False):
@@ -272,8 +280,7 @@ def run_ours(args):
     mv, ms, total_ms = e.step_profiled(K_steps)
     torch.cuda.synchronize(device)
     barrier(dist, device)
-    t_max = max_over_ranks(total_ms, dist, device)
-    value = world * dof_step * K_steps / (t_max * 1e-3)
+    value, t_max = weak_scaling_value(dof_step, K_steps, total_ms, world, dist, device)
 
     # per-kernel roofline (algorithmic bytes per launch / mean launch time)
     S, Kel, wsz = w.shots, w.K, 4

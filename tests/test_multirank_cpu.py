@@ -1,0 +1,69 @@
+"""The benchmark's multi-rank logic on CPU: two gloo ranks, no GPU.
+
+Each rank owns an independent 64-shot batch (sources shifted per rank); the whole-job value is
+every rank's DOF-updates over the slowest rank's time, combined with one MAX all-reduce; the
+reference arm runs on rank 0 only.
+"""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    local_ms = 10.0 * (rank + 1)
+    value, t_max = bench.weak_scaling_value(1000.0, 5, local_ms, world, dist, "cpu")
+    w = bench.WORKLOADS["multishot"][0](10, rank)
+    out[rank] = (value, t_max, float(w.src[0, 0]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_ranks_weak_scaling_and_distinct_shots():
+    world = 2
+    mgr = mp.Manager()
+    out = mgr.dict()
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    v0, t0, x0 = out[0]
+    v1, t1, x1 = out[1]
+    assert t0 == t1 == 20.0                       # max over ranks
+    assert v0 == v1 == pytest.approx(2 * 1000.0 * 5 / 0.020)
+    assert x0 != x1                               # each rank advances its own shot set
+
+
+def test_reference_arm_is_rank0_only(monkeypatch):
+    sys.path.insert(0, ROOT)
+    import bench
+    monkeypatch.setenv("WORLD_SIZE", "1")
+    monkeypatch.setenv("RANK", "1")
+    args = bench.argparse.Namespace(gpus=2, steps=1, warmup=3, impl="reference", workload="square",
+                                    no_cpu_baseline=False)
+    assert bench.run_reference_arm(args) == 0     # returns before any work on a non-zero rank

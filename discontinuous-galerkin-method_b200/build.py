@@ -20,7 +20,7 @@ HOST_SO = os.path.join(PKG, "libdg_host.so")
 GPU_SO = os.path.join(PKG, "libdg_gpu.so")
 
 HOST_SRC = [os.path.join(CSRC, "dg_host.c")]
-GPU_SRC = [os.path.join(CSRC, "dg_gpu.cu")]
+GPU_SRC = [os.path.join(CSRC, "dg_gpu.cu"), os.path.join(CSRC, "dg_noalloc.cu")]
 GPU_DEPS = GPU_SRC + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + \
     [os.path.join(INCLUDE, "dg_gpu.h")]
 

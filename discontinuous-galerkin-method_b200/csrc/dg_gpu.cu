@@ -60,6 +60,10 @@ struct DevBuf {
 
 }  // namespace
 
+namespace dg {
+void set_last_error(const char* msg) { g_last = msg ? msg : ""; }
+}
+
 struct MeshHostInfo {
   long K = 0;
   int Kp = 0, S = 0, n_rec = 0;

@@ -35,7 +35,18 @@ def _ptr(a):
 EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_timed", "dg_gpu_step_profiled",
            "dg_gpu_fetch_traces", "dg_gpu_fetch", "dg_gpu_load",
            "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_steps_done",
-           "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error"]
+           "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error", "dg_gpu_energy_noalloc"]
+
+
+def energy_noalloc(device: int, K: int, fields, jacobi, A, inverV: np.ndarray, out, stream=None) -> None:
+    """dg_gpu_energy_noalloc through the C ABI.
+
+    ``fields`` (Vx, Vz, Txx, Tzz, Txz), ``jacobi``, ``A`` and ``out`` are device buffers the
+    caller owns (anything with ``data_ptr()``); ``inverV`` is a host array.  Nothing is allocated.
+    """
+    iv = np.ascontiguousarray(inverV, dtype=np.float64)
+    ptrs = [f.data_ptr() for f in fields] + [jacobi.data_ptr(), A.data_ptr(), iv.ctypes.data, out.data_ptr()]
+    _check(lib().dg_gpu_energy_noalloc(int(device), int(K), *ptrs, stream), "dg_gpu_energy_noalloc")
 
 
 class DGError(RuntimeError):
@@ -83,6 +94,8 @@ def lib(path: str | None = None):
         L.dg_gpu_step_profiled.restype = C.c_int
         L.dg_gpu_fetch_traces.argtypes = [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p, C.c_void_p]
         L.dg_gpu_fetch_traces.restype = C.c_int
+        L.dg_gpu_energy_noalloc.argtypes = [C.c_int, C.c_long] + [C.c_void_p] * 10
+        L.dg_gpu_energy_noalloc.restype = C.c_int
         L.dg_gpu_fetch.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.dg_gpu_load.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.dg_gpu_reset.argtypes = [C.c_void_p]

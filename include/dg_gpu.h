@@ -151,6 +151,31 @@ int dg_gpu_set_wavelet(dg_gpu_ctx *ctx, int mesh, long t0, long n, const double 
 /* Write a buffer larger than L2 on the context stream (timing hygiene between measurements). */
 int dg_gpu_flush_l2(dg_gpu_ctx *ctx);
 
+/* Largest mesh dg_gpu_energy_noalloc accepts: its scratch holds one partial sum per 256 elements. */
+#define DG_NOALLOC_MAX_ELEMENTS 4194304L
+
+/* Energy of one wavefield, computed without allocating any device memory.
+ * This entry point has no counterpart in the reference.  It serves callers that cannot call
+ * cudaMalloc: for example an energy monitor called from inside another program's time loop,
+ * where that program owns all device memory through its own pool and where a cudaMalloc or
+ * cudaFree would synchronise the device and stall the running solver.
+ * The caller passes every input and the output as device memory of `device`: the five fields
+ * in the reference's layout (double[K][6] each), Jacobi[K] (Jacobian) and A[K][5] (Elastic_A_B:
+ * 1/rho, 1/rho, lambda+2mu, lambda, mu); inverV is a host double[6][6] (inverV.txt); `out`
+ * receives one double, the same quantity dg_gpu_fetch(..., DG_ENERGY, ...) returns.
+ * Scratch: a file-scope static device array of DG_NOALLOC_MAX_ELEMENTS/256 doubles (128 KiB),
+ * which every GPU that loads this library holds until the process exits.  K beyond
+ * DG_NOALLOC_MAX_ELEMENTS is rejected with DG_ERR_ARG before anything runs.  The first call on a
+ * device makes that device current and looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU (other streams, other host threads) race and give
+ * wrong results.  Each call overwrites every partial it reads, so nothing has to start at zero.
+ * `stream` is a cudaStream_t (NULL: the default stream); the call returns after the result is
+ * in `out`. */
+int dg_gpu_energy_noalloc(int device, long K, const double *Vx, const double *Vz, const double *Txx,
+                          const double *Tzz, const double *Txz, const double *Jacobi, const double *A,
+                          const double *inverV, double *out, void *stream);
+
 int dg_gpu_stats_get(dg_gpu_ctx *ctx, dg_gpu_stats *out);
 long dg_gpu_steps_done(dg_gpu_ctx *ctx);
 int dg_gpu_free(dg_gpu_ctx *ctx);

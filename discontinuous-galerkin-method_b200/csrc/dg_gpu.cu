@@ -98,6 +98,8 @@ struct dg_gpu_ctx {
   size_t flush_bytes = 0;
   Ops<double> ops_d{};
   Ops<float> ops_f{};
+  Ops2 ops2{};
+  int x2 = 0;  // shot count of the two-shot FP32 kernels in use (element-major layout), 0: none
   int block = 256;
   int blocks_v = 0, blocks_t = 0;
   bool multi = false;
@@ -321,6 +323,13 @@ int upload_mesh(dg_gpu_ctx* c, const dg_gpu_mesh& m, Prepared& p, MeshDev<R>& d)
   d.S = p.S;
   d.n_rec = p.n_rec;
   d.P = (long long)p.Kp * p.S;
+  if (c->x2) {  // element-major: U[e][plane][S]
+    d.ES = 30LL * p.S;
+    d.PS = p.S;
+  } else {      // plane-major: U[plane][e*S + s]
+    d.ES = p.S;
+    d.PS = d.P;
+  }
   d.steps = m.n_steps;
   d.dt = (R)m.dt;
   d.sponge_elems = (int)p.sponge_elems;
@@ -406,7 +415,8 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
   std::vector<int2> bv, bt;
   for (size_t k = 0; k < md.size(); k++) {
     MeshHostInfo& h = c->mi[k];
-    h.elem_blocks = (int)(((long long)h.K * h.S + B - 1) / B);
+    const long long lanes = c->x2 ? (long long)h.K * (h.S / 2) : (long long)h.K * h.S;
+    h.elem_blocks = (int)((lanes + B - 1) / B);
     h.rec_blocks = (h.n_rec * h.S + B - 1) / B;
     md[k].n_elem_blocks = h.elem_blocks;
     for (int b = 0; b < h.elem_blocks; b++) bv.push_back(make_int2((int)k, b));
@@ -425,6 +435,28 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
     if (rc) return rc;
     rc = c->upload(&c->d_btab_t, bt);
     if (rc) return rc;
+  }
+  return DG_OK;
+}
+
+// shot counts with a two-shot FP32 kernel instance
+bool x2_supported(int S) { return S == 2 || S == 4 || S == 8 || S == 16 || S == 32 || S == 64 || S == 128; }
+
+template <bool KAHAN>
+int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid) {
+  const dim3 bl(c->block), gv(c->blocks_v), gt(c->blocks_t);
+  cudaStream_t st = c->stream;
+  switch (c->x2) {
+#define DG_X2(SS)                                                                      \
+  case SS:                                                                             \
+    k_velocity_x2<SS, KAHAN><<<gv, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);       \
+    if (mid) CK(cudaEventRecord(mid, st));                                             \
+    k_stress_x2<SS, KAHAN><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);         \
+    break;
+    DG_X2(2) DG_X2(4) DG_X2(8) DG_X2(16) DG_X2(32) DG_X2(64) DG_X2(128)
+#undef DG_X2
+    default:
+      return fail(DG_ERR_UNSUPPORTED, "no two-shot kernel for this shot count");
   }
   return DG_OK;
 }
@@ -454,6 +486,9 @@ int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid =
       if (mid) CK(cudaEventRecord(mid, st));
       k_stress<double, false, false><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
     }
+  } else if (c->x2) {
+    int rc = c->kahan ? launch_x2<true>(c, mid) : launch_x2<false>(c, mid);
+    if (rc) return rc;
   } else if (c->kahan) {
     if (c->multi) {
       k_velocity<float, true, true><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_ctr);
@@ -631,6 +666,13 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   c->kahan = o.precision == DG_FP32_KAHAN;
   c->multi = n_meshes > 1;
   c->watchdog_every = std::max(0, o.watchdog_every);
+  {
+    const int S0 = meshes[0].n_shots;
+    const bool fits = (long long)meshes[0].K * (S0 / 2) < (1LL << 31);
+    if (!c->multi && !c->is_double && o.variant != 1 && x2_supported(S0) && fits) c->x2 = S0;
+    if (o.variant == 2 && !c->x2)
+      return fail(DG_ERR_UNSUPPORTED, "the two-shot kernels need one FP32 mesh with 2, 4, ..., 128 shots");
+  }
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   for (auto& e : c->ev) CK(cudaEventCreate(&e));
 
@@ -672,6 +714,11 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   c->stats.bytes_per_step = bytes;
   c->stats.dof_per_step = dof;
   if (c->is_double) fill_ops(c->ops_d, meshes[0]); else fill_ops(c->ops_f, meshes[0]);
+  for (int q = 0; q < 36; q++) {
+    c->ops2.Dr[q] = make_float2(c->ops_f.Dr[q], c->ops_f.Dr[q]);
+    c->ops2.Ds[q] = make_float2(c->ops_f.Ds[q], c->ops_f.Ds[q]);
+  }
+  for (int q = 0; q < 54; q++) c->ops2.L[q] = make_float2(c->ops_f.L[q], c->ops_f.L[q]);
   int rc;
   if ((rc = c->alloc(&c->d_ctr, 1))) return rc;
   if ((rc = c->alloc(&c->d_flag, 1))) return rc;
@@ -733,7 +780,7 @@ static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
     if (c->watchdog_every > 0 && c->t % c->watchdog_every == 0) {
       CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
       for (size_t k = 0; k < c->mi.size(); k++) {
-        const long long nvals = 12LL * c->mi[k].Kp * c->mi[k].S;
+        const long long nvals = 30LL * c->mi[k].Kp * c->mi[k].S;
         if (c->is_double) k_nonfinite<double><<<592, 256, 0, c->stream>>>(c->md_d[k].U, nvals, c->d_flag);
         else k_nonfinite<float><<<592, 256, 0, c->stream>>>(c->md_f[k].U, nvals, c->d_flag);
         c->stats.launches++;
@@ -845,10 +892,10 @@ int dg_gpu_fetch(dg_gpu_ctx* c, int what, int mesh, int shot, double* dst) {
     const long long n = h.K * 6;
     const int grid = (int)((n + B - 1) / B);
     if (c->is_double)
-      k_fetch_field<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].U, what * 6, c->md_d[mesh].P, h.S, shot,
+      k_fetch_field<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].U, what * 6, c->md_d[mesh].ES, c->md_d[mesh].PS, shot,
                                                        h.d_new_of_old, (int)h.K, c->d_stage);
     else
-      k_fetch_field<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].U, what * 6, c->md_f[mesh].P, h.S, shot,
+      k_fetch_field<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].U, what * 6, c->md_f[mesh].ES, c->md_f[mesh].PS, shot,
                                                       h.d_new_of_old, (int)h.K, c->d_stage);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(dst, c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -889,10 +936,10 @@ int dg_gpu_load(dg_gpu_ctx* c, int what, int mesh, int shot, const double* src) 
   CK(cudaMemcpyAsync(c->d_stage, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   const int B = 256, grid = (int)((n + B - 1) / B);
   if (c->is_double)
-    k_load_field<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].U, c->md_d[mesh].C, what * 6, c->md_d[mesh].P, h.S,
+    k_load_field<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].U, c->md_d[mesh].C, what * 6, c->md_d[mesh].ES, c->md_d[mesh].PS,
                                                     shot, h.d_new_of_old, (int)h.K, c->d_stage);
   else
-    k_load_field<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].U, c->md_f[mesh].C, what * 6, c->md_f[mesh].P, h.S,
+    k_load_field<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].U, c->md_f[mesh].C, what * 6, c->md_f[mesh].ES, c->md_f[mesh].PS,
                                                    shot, h.d_new_of_old, (int)h.K, c->d_stage);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));

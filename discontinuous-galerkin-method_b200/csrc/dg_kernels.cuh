@@ -45,7 +45,8 @@ template <class R> struct Ops {
 };
 
 template <class R> struct MeshDev {
-  long long P;            // plane stride Kp * S
+  long long P;            // plane stride of the plane-major layout (Kp * S)
+  long long ES, PS;       // value (e, plane, s) lives at U[e*ES + plane*PS + s] in either layout
   long long steps;        // this mesh's wavelet length
   int K, Kp, S, n_rec;
   int n_elem_blocks;      // element blocks of this mesh (grid = these + recorder blocks)
@@ -276,10 +277,10 @@ __device__ __forceinline__ void record(const MeshDev<R>& m, int lb_rec, long lon
   if (q >= m.n_rec * S) return;
   const int r = q / S, s = q - r * S;
   const int e = __ldg(m.rec_elem + r), node = __ldg(m.rec_node + r);
-  const long long at = (long long)e * S + s;
+  const long long at = (long long)e * m.ES + s;
   R* tr = m.trace + (t * 2) * (long long)m.n_rec * S;
-  tr[q] = m.U[(0 + node) * m.P + at];
-  tr[(long long)m.n_rec * S + q] = m.U[(6 + node) * m.P + at];
+  tr[q] = m.U[at + (0 + node) * m.PS];
+  tr[(long long)m.n_rec * S + q] = m.U[at + (6 + node) * m.PS];
 }
 
 // Stress half-step, geometric-factor form: T = a T + dt L_T(V) (OpenMP_Function.c:188-306),
@@ -648,27 +649,357 @@ __global__ void __launch_bounds__(256) k_stress_ref(const __grid_constant__ Ops<
 }
 
 // -------------------------------------------------------------------------------------------
+// Two-shot FP32 kernels for even shot counts, on Blackwell's packed FP32x2 arithmetic
+// (__ffma2_rn / __fmul2_rn / __fadd2_rn: one instruction advances two shots).  Layout:
+// element-major with shots innermost, U[e][plane][S], so thread q of an element owns shots 2q and
+// 2q+1 as one float2 and all 30 planes of its element sit at compile-time offsets (multiples of
+// S/2 float2) from one base address; a neighbour's planes likewise from nb * 30 * S/2.  The
+// operator constants come pre-duplicated as float2 pairs so they feed the packed FMAs directly.
+struct Ops2 {
+  float2 Dr[NP * NP];
+  float2 Ds[NP * NP];
+  float2 L[NF * NP * NF];
+};
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b, exactly rounded (b * -1 is exact)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+
+// Kahan-compensated u += d with compensation c (both lanes)
+__device__ __forceinline__ void kahan2(float2& u, float2& c, float2 d) {
+  const float2 y = sub2(d, c);
+  const float2 t = add2(u, y);
+  c = sub2(sub2(t, u), y);
+  u = t;
+}
+
+template <int S, bool KAHAN>
+__global__ void __launch_bounds__(256, 2) k_velocity_x2(const __grid_constant__ Ops2 ops,
+                                                        const __grid_constant__ MeshDev<float> m,
+                                                        Counters* __restrict__ ctr) {
+  constexpr int H = S / 2;    // float2 lanes per element
+  constexpr int ES = 30 * H;  // element stride in float2
+  const long long t = ctr->v;
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
+  if (t >= m.steps) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= m.K * H) return;
+  const int e = g / H, q = g - e * H;
+  float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * ES + q;
+
+  float2 txx[NP], tzz[NP], txz[NP];
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    txx[i] = Ue[(12 + i) * H];
+    tzz[i] = Ue[(18 + i) * H];
+    txz[i] = Ue[(24 + i) * H];
+  }
+  const int4 fc = __ldg(m.face + e);
+  const float4 gm = __ldg(m.geo + e);
+  const float irho = __ldg(&m.mat[e].x);
+  const bool own_sponge = fc.w & 1;
+  if (own_sponge) {
+#pragma unroll
+    for (int i = 0; i < NP; i++) {
+      const float2 a = f2(__ldg(m.sponge + (long long)i * m.Kp + e));
+      txx[i] = mul2(txx[i], a); tzz[i] = mul2(tzz[i], a); txz[i] = mul2(txz[i], a);
+    }
+  }
+  float2 hx[NP], hz[NP];
+#pragma unroll
+  for (int i = 0; i < NP; i++) { hx[i] = f2(0.f); hz[i] = f2(0.f); }
+
+  // surface terms: sum_j S_j (nx_j dTxx + nz_j dTxz), sum_j S_j (nz_j dTzz + nx_j dTxz)
+  const int codes[3] = {fc.x, fc.y, fc.z};
+#pragma unroll
+  for (int j = 0; j < NF; j++) {
+    const int code = codes[j];
+    float nxs, nzs;
+    if (j == 0) { nxs = -0.5f * gm.y; nzs = -0.5f * gm.w; }
+    else if (j == 1) { nxs = 0.5f * (gm.x + gm.y); nzs = 0.5f * (gm.z + gm.w); }
+    else { nxs = -0.5f * gm.x; nzs = -0.5f * gm.z; }
+    const float2 nx = f2(nxs), nz = f2(nzs);
+    float2 pxx[NF], pzz[NF], pxz[NF];
+    if (code < 0) {
+#pragma unroll
+      for (int k = 0; k < NF; k++) { pxx[k] = f2(0.f); pzz[k] = f2(0.f); pxz[k] = f2(0.f); }
+    } else {
+      const int nb = code >> 4, nf = (code >> 1) & 3, flip = code & 1;
+      const float2* __restrict__ Un = reinterpret_cast<const float2*>(m.U) + (long long)nb * ES + q;
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        const int node = face_node(nf, flip ? 2 - k : k);
+        pxx[k] = Un[(12 + node) * H];
+        pzz[k] = Un[(18 + node) * H];
+        pxz[k] = Un[(24 + node) * H];
+      }
+      if (code & 8) {
+#pragma unroll
+        for (int k = 0; k < NF; k++) {
+          const int node = face_node(nf, flip ? 2 - k : k);
+          const float2 a = f2(__ldg(m.sponge + (long long)node * m.Kp + nb));
+          pxx[k] = mul2(pxx[k], a); pzz[k] = mul2(pzz[k], a); pxz[k] = mul2(pxz[k], a);
+        }
+      }
+    }
+    float2 fx[NF], fz[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      const int own = face_node(j, k);
+      const float2 dxx = sub2(pxx[k], txx[own]);
+      const float2 dzz = sub2(pzz[k], tzz[own]);
+      const float2 dxz = sub2(pxz[k], txz[own]);
+      fx[k] = fma2(nx, dxx, mul2(nz, dxz));
+      fz[k] = fma2(nz, dzz, mul2(nx, dxz));
+    }
+#pragma unroll
+    for (int i = 0; i < NP; i++)
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        hx[i] = fma2(ops.L[(j * NP + i) * NF + k], fx[k], hx[i]);
+        hz[i] = fma2(ops.L[(j * NP + i) * NF + k], fz[k], hz[i]);
+      }
+  }
+
+  // volume terms: Dr (rx Txx + rz Txz) + Ds (sx Txx + sz Txz) and the same for (Txz, Tzz)
+  const float2 rx = f2(gm.x), sx = f2(gm.y), rz = f2(gm.z), sz = f2(gm.w);
+  {
+    float2 a[NP], b[NP];
+#pragma unroll
+    for (int n = 0; n < NP; n++) {
+      a[n] = fma2(rx, txx[n], mul2(rz, txz[n]));
+      b[n] = fma2(sx, txx[n], mul2(sz, txz[n]));
+    }
+#pragma unroll
+    for (int i = 0; i < NP; i++)
+#pragma unroll
+      for (int n = 0; n < NP; n++) {
+        hx[i] = fma2(ops.Dr[i * NP + n], a[n], hx[i]);
+        hx[i] = fma2(ops.Ds[i * NP + n], b[n], hx[i]);
+      }
+  }
+  {
+    float2 a[NP], b[NP];
+#pragma unroll
+    for (int n = 0; n < NP; n++) {
+      a[n] = fma2(rx, txz[n], mul2(rz, tzz[n]));
+      b[n] = fma2(sx, txz[n], mul2(sz, tzz[n]));
+    }
+#pragma unroll
+    for (int i = 0; i < NP; i++)
+#pragma unroll
+      for (int n = 0; n < NP; n++) {
+        hz[i] = fma2(ops.Dr[i * NP + n], a[n], hz[i]);
+        hz[i] = fma2(ops.Ds[i * NP + n], b[n], hz[i]);
+      }
+  }
+
+  // V = a V (+ source on Vz) + dt/rho * rhs
+  float2 vx[NP], vz[NP], cx[NP], cz[NP];
+#pragma unroll
+  for (int i = 0; i < NP; i++) { vx[i] = Ue[(0 + i) * H]; vz[i] = Ue[(6 + i) * H]; }
+  float2* __restrict__ Ce = nullptr;
+  if (KAHAN) {
+    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * ES + q;
+#pragma unroll
+    for (int i = 0; i < NP; i++) { cx[i] = Ce[(0 + i) * H]; cz[i] = Ce[(6 + i) * H]; }
+  }
+  if (own_sponge) {
+#pragma unroll
+    for (int i = 0; i < NP; i++) {
+      const float2 a = f2(__ldg(m.sponge + (long long)i * m.Kp + e));
+      vx[i] = mul2(vx[i], a); vz[i] = mul2(vz[i], a);
+      if (KAHAN) { cx[i] = mul2(cx[i], a); cz[i] = mul2(cz[i], a); }
+    }
+  }
+  const int2 se = __ldg(reinterpret_cast<const int2*>(m.src_elem) + q);
+  float2 src[NP];
+#pragma unroll
+  for (int i = 0; i < NP; i++) src[i] = f2(0.f);
+  if (se.x == e || se.y == e) {
+    const float w = (float)__ldg(m.wavelet + t);
+#pragma unroll
+    for (int i = 0; i < NP; i++) {
+      src[i].x = se.x == e ? __ldg(m.src_fun + (2 * q) * NP + i) * w : 0.f;
+      src[i].y = se.y == e ? __ldg(m.src_fun + (2 * q + 1) * NP + i) * w : 0.f;
+    }
+  }
+  const float2 step = f2(m.dt * irho);
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    if (KAHAN) {
+      kahan2(vx[i], cx[i], mul2(step, hx[i]));
+      kahan2(vz[i], cz[i], fma2(step, hz[i], src[i]));
+    } else {
+      vx[i] = fma2(step, hx[i], vx[i]);
+      vz[i] = fma2(step, hz[i], add2(vz[i], src[i]));
+    }
+    Ue[(0 + i) * H] = vx[i];
+    Ue[(6 + i) * H] = vz[i];
+  }
+  if (KAHAN) {
+#pragma unroll
+    for (int i = 0; i < NP; i++) { Ce[(0 + i) * H] = cx[i]; Ce[(6 + i) * H] = cz[i]; }
+  }
+}
+
+template <int S, bool KAHAN>
+__global__ void __launch_bounds__(256, 2) k_stress_x2(const __grid_constant__ Ops2 ops,
+                                                      const __grid_constant__ MeshDev<float> m,
+                                                      Counters* __restrict__ ctr) {
+  constexpr int H = S / 2;
+  constexpr int ES = 30 * H;
+  const long long t = ctr->s;
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
+  if (t >= m.steps) return;
+  if ((int)blockIdx.x >= m.n_elem_blocks) { record(m, blockIdx.x - m.n_elem_blocks, t); return; }
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= m.K * H) return;
+  const int e = g / H, q = g - e * H;
+  float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * ES + q;
+
+  float2 vx[NP], vz[NP];
+#pragma unroll
+  for (int i = 0; i < NP; i++) { vx[i] = Ue[(0 + i) * H]; vz[i] = Ue[(6 + i) * H]; }
+  const int4 fc = __ldg(m.face + e);
+  const float4 gm = __ldg(m.geo + e);
+  const float4 mt = __ldg(m.mat + e);
+  const float2 rx = f2(gm.x), sx = f2(gm.y), rz = f2(gm.z), sz = f2(gm.w);
+
+  // volume: X = dxVx, Z = dzVz, W = dxVz + dzVx
+  float2 X[NP], Z[NP], W[NP];
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    float2 drx = f2(0.f), dsx = f2(0.f), drz = f2(0.f), dsz = f2(0.f);
+#pragma unroll
+    for (int n = 0; n < NP; n++) {
+      drx = fma2(ops.Dr[i * NP + n], vx[n], drx);
+      dsx = fma2(ops.Ds[i * NP + n], vx[n], dsx);
+      drz = fma2(ops.Dr[i * NP + n], vz[n], drz);
+      dsz = fma2(ops.Ds[i * NP + n], vz[n], dsz);
+    }
+    X[i] = fma2(rx, drx, mul2(sx, dsx));
+    Z[i] = fma2(rz, drz, mul2(sz, dsz));
+    W[i] = fma2(rx, drz, fma2(sx, dsz, fma2(rz, drx, mul2(sz, dsx))));
+  }
+
+  const int codes[3] = {fc.x, fc.y, fc.z};
+#pragma unroll
+  for (int j = 0; j < NF; j++) {
+    const int code = codes[j];
+    float nxs, nzs;
+    if (j == 0) { nxs = -0.5f * gm.y; nzs = -0.5f * gm.w; }
+    else if (j == 1) { nxs = 0.5f * (gm.x + gm.y); nzs = 0.5f * (gm.z + gm.w); }
+    else { nxs = -0.5f * gm.x; nzs = -0.5f * gm.z; }
+    const float2 nx = f2(nxs), nz = f2(nzs);
+    float2 px[NF], pz[NF];
+    if (code < 0) {
+#pragma unroll
+      for (int k = 0; k < NF; k++) { px[k] = f2(0.f); pz[k] = f2(0.f); }
+    } else {
+      const int nb = code >> 4, nf = (code >> 1) & 3, flip = code & 1;
+      const float2* __restrict__ Un = reinterpret_cast<const float2*>(m.U) + (long long)nb * ES + q;
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        const int node = face_node(nf, flip ? 2 - k : k);
+        px[k] = Un[(0 + node) * H];
+        pz[k] = Un[(6 + node) * H];
+      }
+    }
+    float2 fa[NF], fb[NF], fw[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      const int own = face_node(j, k);
+      const float2 dvx = sub2(px[k], vx[own]);
+      const float2 dvz = sub2(pz[k], vz[own]);
+      fa[k] = mul2(nx, dvx);
+      fb[k] = mul2(nz, dvz);
+      fw[k] = fma2(nz, dvx, mul2(nx, dvz));
+    }
+#pragma unroll
+    for (int i = 0; i < NP; i++)
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        const float2 l = ops.L[(j * NP + i) * NF + k];
+        X[i] = fma2(l, fa[k], X[i]);
+        Z[i] = fma2(l, fb[k], Z[i]);
+        W[i] = fma2(l, fw[k], W[i]);
+      }
+  }
+
+  float2 txx[NP], tzz[NP], txz[NP], cxx[NP], czz[NP], cxz[NP];
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    txx[i] = Ue[(12 + i) * H];
+    tzz[i] = Ue[(18 + i) * H];
+    txz[i] = Ue[(24 + i) * H];
+  }
+  float2* __restrict__ Ce = nullptr;
+  if (KAHAN) {
+    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * ES + q;
+#pragma unroll
+    for (int i = 0; i < NP; i++) { cxx[i] = Ce[(12 + i) * H]; czz[i] = Ce[(18 + i) * H]; cxz[i] = Ce[(24 + i) * H]; }
+  }
+  if (fc.w & 1) {
+#pragma unroll
+    for (int i = 0; i < NP; i++) {
+      const float2 a = f2(__ldg(m.sponge + (long long)i * m.Kp + e));
+      txx[i] = mul2(txx[i], a); tzz[i] = mul2(tzz[i], a); txz[i] = mul2(txz[i], a);
+      if (KAHAN) { cxx[i] = mul2(cxx[i], a); czz[i] = mul2(czz[i], a); cxz[i] = mul2(cxz[i], a); }
+    }
+  }
+  const float2 dl2m = f2(m.dt * mt.w), dlam = f2(m.dt * mt.y), dmu = f2(m.dt * mt.z);
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    const float2 dxx = fma2(dl2m, X[i], mul2(dlam, Z[i]));
+    const float2 dzz = fma2(dlam, X[i], mul2(dl2m, Z[i]));
+    const float2 dxz = mul2(dmu, W[i]);
+    if (KAHAN) {
+      kahan2(txx[i], cxx[i], dxx);
+      kahan2(tzz[i], czz[i], dzz);
+      kahan2(txz[i], cxz[i], dxz);
+    } else {
+      txx[i] = add2(txx[i], dxx);
+      tzz[i] = add2(tzz[i], dzz);
+      txz[i] = add2(txz[i], dxz);
+    }
+    Ue[(12 + i) * H] = txx[i];
+    Ue[(18 + i) * H] = tzz[i];
+    Ue[(24 + i) * H] = txz[i];
+  }
+  if (KAHAN) {
+#pragma unroll
+    for (int i = 0; i < NP; i++) {
+      Ce[(12 + i) * H] = cxx[i]; Ce[(18 + i) * H] = czz[i]; Ce[(24 + i) * H] = cxz[i];
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------------
 // Layout conversions and diagnostics.
 
 // internal [plane][e*S+s] (locality order) -> reference element-major double[K][6]
 template <class R>
-__global__ void k_fetch_field(const R* __restrict__ U, int plane0, long long P, int S, int s,
+__global__ void k_fetch_field(const R* __restrict__ U, int plane0, long long ES, long long PS, int s,
                               const int* __restrict__ new_of_old, int K, double* __restrict__ out) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= (long long)K * NP) return;
   const int eo = (int)(q / NP), i = (int)(q - (long long)eo * NP);
   const int en = __ldg(new_of_old + eo);
-  out[q] = (double)U[(plane0 + i) * P + (long long)en * S + s];
+  out[q] = (double)U[(long long)en * ES + (plane0 + i) * PS + s];
 }
 
 template <class R>
-__global__ void k_load_field(R* __restrict__ U, R* __restrict__ C, int plane0, long long P, int S, int s,
+__global__ void k_load_field(R* __restrict__ U, R* __restrict__ C, int plane0, long long ES, long long PS, int s,
                              const int* __restrict__ new_of_old, int K, const double* __restrict__ in) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= (long long)K * NP) return;
   const int eo = (int)(q / NP), i = (int)(q - (long long)eo * NP);
   const int en = __ldg(new_of_old + eo);
-  const long long at = (plane0 + i) * P + (long long)en * S + s;
+  const long long at = (long long)en * ES + (plane0 + i) * PS + s;
   U[at] = (R)in[q];
   if (C) C[at] = R(0);
 }
@@ -711,12 +1042,12 @@ __global__ void k_energy(const __grid_constant__ Ops<R> ops, const __grid_consta
     const double rx = gm.x, sx = gm.y, rz = gm.z, sz = gm.w;
     const double J = 1.0 / (rx * sz - sx * rz);
     const double rho = 1.0 / (double)mt.x, lam = mt.y, mu = mt.z;
-    const long long g = (long long)e * m.S + s;
+    const long long g = (long long)e * m.ES + s;
     double f[5][NP];
 #pragma unroll
     for (int c = 0; c < 5; c++)
 #pragma unroll
-      for (int i = 0; i < NP; i++) f[c][i] = (double)m.U[(c * NP + i) * m.P + g];
+      for (int i = 0; i < NP; i++) f[c][i] = (double)m.U[g + (c * NP + i) * m.PS];
     const double det = 4.0 * mu * (lam + mu);
 #pragma unroll
     for (int i = 0; i < NP; i++)

@@ -69,7 +69,7 @@ class _Mesh(C.Structure):
 class _Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("reorder", C.c_int), ("block_threads", C.c_int),
                 ("graph_steps", C.c_int), ("autotune", C.c_int), ("watchdog_every", C.c_int),
-                ("tune_cache", C.c_char_p)]
+                ("tune_cache", C.c_char_p), ("variant", C.c_int)]
 
 
 class _Stats(C.Structure):
@@ -149,7 +149,7 @@ class Engine:
     """One device context over one or more meshes (all meshes step together)."""
 
     def __init__(self, meshes, precision="fp64", *, device=0, reorder=True, block_threads=0, graph_steps=0,
-                 autotune=False, watchdog_every=0, tune_cache=None):
+                 autotune=False, watchdog_every=0, tune_cache=None, variant=0):
         if isinstance(meshes, dict):
             meshes = [meshes]
         prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
@@ -187,6 +187,7 @@ class Engine:
         opts.autotune = 1 if autotune else 0
         opts.watchdog_every = watchdog_every
         opts.tune_cache = tune_cache.encode() if tune_cache else None
+        opts.variant = int(variant)
         self._ctx = C.c_void_p()
         _check(lib().dg_gpu_init(C.byref(self._ctx), arr, len(meshes), C.byref(opts)), "dg_gpu_init")
         self._keep = []

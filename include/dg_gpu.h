@@ -95,6 +95,8 @@ typedef struct {
 	int autotune;        /* 1: time candidate block sizes at init */
 	int watchdog_every;  /* check the velocity fields for NaN/Inf every k steps (0: off) */
 	const char *tune_cache; /* file that keeps autotune results between runs (NULL: none) */
+	int variant;         /* FP32 kernels: 0 automatic, 1 one shot per thread (plane-major layout),
+	                        2 two shots per thread with packed FP32x2 (needs n_shots in {2,4,...,128}) */
 } dg_gpu_opts;
 
 typedef struct {

@@ -214,6 +214,61 @@ def test_invalid_maps_rejected_on_host():
     assert ei.value.code == -9
 
 
+def _repeat_shots(a, S, pattern=(0, 1, 2)):
+    """Mesh dict with S shots cycling through the fixture's shots."""
+    m = eng.mesh_from_setup(a)
+    idx = [pattern[i % len(pattern)] for i in range(S)]
+    m["source"] = np.ascontiguousarray(a["source"].reshape(-1, 2)[idx])
+    m["fun"] = np.ascontiguousarray(a["fun"].reshape(-1, 6)[idx])
+    return m, idx
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp32_kahan"])
+@pytest.mark.parametrize("S", [2, 4, 64])
+def test_two_shot_kernels_against_reference(precision, S):
+    """Packed FP32x2 kernels (element-major layout) against the reference's traces."""
+    g = Golden("square_3shots")
+    m, idx = _repeat_shots(g.setup_arrays(), S)
+    with eng.Engine(m, precision, variant=2) as e:
+        e.step(g.steps)
+        for s in (0, 1, S - 1):
+            ref = np.concatenate([g.z["shot%d_rec_x" % idx[s]], g.z["shot%d_rec_z" % idx[s]]])
+            got = np.concatenate([e.fetch("trace_x", 0, s), e.fetch("trace_z", 0, s)])
+            assert rel_l2(got, ref) <= 1e-4, (s, rel_l2(got, ref))
+            assert rel_l2(e.fetch("Txz", 0, s), g.z["shot%d_final_Txz" % idx[s]]) <= 1e-3
+
+
+def test_two_shot_and_one_shot_kernels_agree():
+    g = Golden("slope_coupled")
+    m, _ = _repeat_shots(g.setup_arrays(), 4, pattern=(0,))
+    out = []
+    for variant in (1, 2):
+        with eng.Engine(m, "fp32", variant=variant) as e:
+            e.step(g.steps)
+            out.append([e.fetch(f, 0, s) for s in range(4) for f in FIELDS] + [e.fetch("trace_z", 0, 3)])
+    for a, b in zip(*out):
+        assert rel_l2(a, b) <= 2e-5
+
+
+def test_two_shot_checkpoint_restore():
+    g = Golden("square_K288")
+    m, _ = _repeat_shots(g.setup_arrays(), 2, pattern=(0,))
+    with eng.Engine(m, "fp32", variant=2) as a, eng.Engine(m, "fp32", variant=2) as b:
+        a.step(80)
+        state = [[a.fetch(f, 0, s) for f in FIELDS] for s in range(2)]
+        a.step(g.steps - 80)
+        b.set_wavelet(0, np.zeros(80))
+        b.step(80)
+        for s in range(2):
+            for f, v in zip(FIELDS, state[s]):
+                b.load(f, v, 0, s)
+        b.step(g.steps - 80)
+        for s in range(2):
+            for f in FIELDS:
+                assert np.array_equal(a.fetch(f, 0, s), b.fetch(f, 0, s))
+            assert np.array_equal(a.fetch("trace_x", 0, s)[80:], b.fetch("trace_x", 0, s)[80:])
+
+
 @pytest.mark.slow
 def test_homogeneous_square_full_size_against_oracle():
     """The 20,000-element square, 400 steps: FP64 within 1e-10 of the oracle, REF bit-exact."""

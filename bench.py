@@ -2,17 +2,18 @@
 """Benchmark of the DG elastic-wave time loop on B200.
 
 One bench step = one time step of the whole workload: sponge, source, velocity half-step,
-stress half-step and receiver record for every element and shot.  The default workload is the
-multi-shot batch: a layered elastic mesh of 200,000 triangles advanced for 64 shots at once in
-FP32 (shots innermost).  Beside it the line reports the plain FP64 path (one shot, L2 flushed
-between steps), the FP32-vs-FP64 trace error, the roofline of the dominant kernel, an
-end-to-end figure through the public API with host buffers, and the reference's own CPU code
-timed on this host.
+stress half-step and receiver record for every element, shot and mesh.  The default workload is
+the multi-shot batch: a layered elastic mesh of 200,000 triangles advanced for 64 shots at once
+in FP32 (shots innermost).  Beside it the line reports the plain FP64 path (one shot, L2 flushed
+between steps), the FP32-vs-FP64 trace error, the roofline of the dominant kernel, an end-to-end
+figure through the public API with host buffers, and the reference's own CPU code timed on this
+host.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+                    [--precision fp32|fp32_kahan|fp64]
 
-Under torchrun (N > 1) every rank advances its own 64-shot batch (shots shifted along the
-surface per rank, no collective on the data path); the time is the maximum over ranks.
+Under torchrun (N > 1) every rank advances its own batch (shots shifted along the surface per
+rank, no collective on the data path); the time is the maximum over ranks.
 """
 from __future__ import annotations
 
@@ -49,8 +50,15 @@ def pkg():
     return importlib.import_module("discontinuous-galerkin-method_b200")
 
 
+def _uneven(steps, rank):
+    ws, _ = pkg().workloads.uneven_batch(seed=5 + 97 * rank)
+    for w in ws:
+        w.steps = steps
+    return ws
+
+
 WORKLOADS = {
-    # name: (constructor(steps, rank), description)
+    # name: (constructor(steps, rank) -> Workload or list of Workloads, description)
     "multishot": (lambda steps, rank: pkg().workloads.layered_multishot(steps=steps, shot_phase=(rank % 16) / 16.0),
                   "multi-shot layered elastic batch: 200,000 triangles x 64 shots"),
     "slope": (lambda steps, rank: pkg().workloads.coupled_slope(steps=steps),
@@ -59,6 +67,7 @@ WORKLOADS = {
                "heterogeneous random medium: 2,000,000 triangles, 1 shot"),
     "square": (lambda steps, rank: pkg().workloads.homogeneous_square(steps=steps),
                "homogeneous square: 20,000 triangles, 1 shot"),
+    "uneven": (_uneven, "uneven batch: 48 meshes, 5,000-500,000 triangles (log-uniform), 1-8 shots each"),
 }
 
 
@@ -143,7 +152,7 @@ def max_over_ranks(x: float, dist, device) -> float:
     return float(t.item())
 
 
-def weak_scaling_value(dof_per_step_per_rank: float, steps: int, local_ms: float, world: int, dist, device) -> float:
+def weak_scaling_value(dof_per_step_per_rank: float, steps: int, local_ms: float, world: int, dist, device):
     """Whole-job DOF-updates/s: every rank's work over the slowest rank's device time."""
     t_max = max_over_ranks(local_ms, dist, device)
     return world * dof_per_step_per_rank * steps / (t_max * 1e-3), t_max
@@ -157,14 +166,22 @@ def barrier(dist, device):
             torch.cuda.synchronize(device)
 
 
-def cpu_reference(w, steps_hint: float = 12.0, force_port: bool = False):
+def as_list(w):
+    return w if isinstance(w, list) else [w]
+
+
+def one_shot(w):
+    return pkg().workloads.Workload(w.name, w.mesh, w.vp, w.vs, w.rho, w.fp, w.sponge, w.src[:1], w.rec, w.steps)
+
+
+def cpu_reference(w, steps_hint: float = 12.0):
     """Time the reference's own OpenMP code (oracle/_ref) on this host: one shot, all cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refrun  # CPU-baseline leg only
 
     cores = os.cpu_count() or 1
-    w1 = pkg().workloads.Workload(w.name, w.mesh, w.vp, w.vs, w.rho, w.fp, w.sponge, w.src[:1], w.rec, w.steps)
-    if refrun.available(w1) and not force_port:
+    w1 = one_shot(w)
+    if refrun.available(w1):
         with tempfile.TemporaryDirectory() as d:
             probe = refrun.run(w1, os.path.join(d, "p"), steps=5, threads=cores, dump_setup=0, work_dir=os.path.join(d, "w"))
             per = probe["timing"]["loop_seconds"] / 5
@@ -188,8 +205,8 @@ def cpu_reference(w, steps_hint: float = 12.0, force_port: bool = False):
         kind = "port"
     dof = 30.0 * w1.K * n
     return {"value": dof / sec, "unit": UNIT, "cores": th, "kind": kind,
-            "sample": "1 of %d shots, first %d time steps, K=%d, OpenMP %d threads, loop time only (%.1f s)"
-                      % (w.shots, n, w1.K, th, sec)}
+            "sample": "1 of %d shots of a %d-triangle mesh, first %d time steps, OpenMP %d threads, loop time only "
+                      "(%.1f s)" % (w.shots, w1.K, n, th, sec)}
 
 
 def run_reference_arm(args):
@@ -197,11 +214,11 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     ctor, desc = WORKLOADS[args.workload]
-    w = ctor(max(args.steps, args.warmup) + 10, 0)
+    w = as_list(ctor(max(args.steps, args.warmup) + 10, 0))[0]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refrun
     cores = os.cpu_count() or 1
-    w1 = pkg().workloads.Workload(w.name, w.mesh, w.vp, w.vs, w.rho, w.fp, w.sponge, w.src[:1], w.rec, w.steps)
+    w1 = one_shot(w)
     with tempfile.TemporaryDirectory() as d:
         if refrun.available(w1):
             if args.warmup:
@@ -226,7 +243,8 @@ def run_reference_arm(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc, "shots_timed": 1, "K": w1.K, "threads": th},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": kind,
-                             "sample": "1 shot, %d time steps after %d warm-up steps" % (args.steps, args.warmup)},
+                             "sample": "1 shot of the first mesh, %d time steps after %d warm-up steps"
+                                       % (args.steps, args.warmup)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -243,6 +261,15 @@ def read_traffic(workload: str, kernel: str):
     except OSError:
         pass
     return None
+
+
+def kernel_bytes(ws, precision):
+    """Algorithmic bytes of one velocity and one stress launch over the batch."""
+    w = 8 if precision.startswith("fp64") else 4
+    comp = precision == "fp32_kahan"
+    bv = sum(x.K * (42 * x.shots * w + (24 * x.shots * 4 if comp else 0) + 5 * w + 16) for x in ws)
+    bs = sum(x.K * (48 * x.shots * w + (36 * x.shots * 4 if comp else 0) + 8 * w + 16) for x in ws)
+    return bv, bs
 
 
 def run_ours(args):
@@ -262,18 +289,17 @@ def run_ours(args):
     e2e_steps = max(e2e_chunk, (K_steps // e2e_chunk) * e2e_chunk)
     acc_steps = 200
     table = max(W_steps + K_steps, W_steps + e2e_steps, acc_steps) + 8
-    w = ctor(table, rank)
-    s = P.host.build_setup(w, full=False, n_steps=table)
-    mesh = eng.mesh_from_setup(s, with_ref_ops=False)
+    ws = as_list(ctor(table, rank))
+    setups = [P.host.build_setup(w, full=False, n_steps=table) for w in ws]
+    meshes = [eng.mesh_from_setup(s, with_ref_ops=False) for s in setups]
     peak, peak_src = peaks()
     sampler = ClockSampler(device)
     sampler.start()
 
-    # ---- headline: batched FP32, inputs resident in HBM ------------------------------------
-    e = eng.Engine(mesh, "fp32", device=device)
+    # ---- headline: the batch in the requested arithmetic, inputs resident in HBM ------------
+    e = eng.Engine(meshes, args.precision, device=device)
     st = e.stats()
-    bytes_step = st["bytes_per_step"]
-    dof_step = st["dof_per_step"]
+    bytes_step, dof_step = st["bytes_per_step"], st["dof_per_step"]
     e.step(W_steps)
     barrier(dist, device)
     torch.cuda.synchronize(device)
@@ -282,85 +308,99 @@ def run_ours(args):
     barrier(dist, device)
     value, t_max = weak_scaling_value(dof_step, K_steps, total_ms, world, dist, device)
 
-    # per-kernel roofline (algorithmic bytes per launch / mean launch time)
-    S, Kel, wsz = w.shots, w.K, 4
-    b_vel = Kel * (42 * S * wsz + 5 * wsz + 16)
-    b_str = Kel * (48 * S * wsz + 8 * wsz + 16)
+    b_vel, b_str = kernel_bytes(ws, args.precision)
     t_vel, t_str = float(np.mean(mv)), float(np.mean(ms))
-    dom = ("k_stress", b_str, t_str) if t_str >= t_vel else ("k_velocity", b_vel, t_vel)
+    names = eng.KERNEL_NAMES[st["kernel_family"]]
+    dom = (names[1], b_str, t_str) if t_str >= t_vel else (names[0], b_vel, t_vel)
     achieved = dom[1] / (dom[2] * 1e-3) / 1e9
     traffic = read_traffic(args.workload, dom[0])
+    S_tot = sum(x.shots for x in ws)
+    K_tot = sum(x.K for x in ws)
+    R_tot = sum(x.shots * x.rec.shape[0] for x in ws)
+    wbytes = 8 if args.precision == "fp64" else 4
+    state_bytes = sum(30 * x.K * x.shots for x in ws) * (wbytes + (4 if args.precision == "fp32_kahan" else 0))
 
     # ---- end to end through the public API with pinned host buffers ------------------------
     e.reset()
     e.step(W_steps)
-    R = w.rec.shape[0]
-    wav = torch.empty(e2e_chunk, dtype=torch.float64).pin_memory()
-    wav.copy_(torch.from_numpy(np.ascontiguousarray(s.arrays["wavelet"][:e2e_chunk])))
-    out_x = torch.empty((S, e2e_chunk, R), dtype=torch.float64).pin_memory()
-    out_z = torch.empty((S, e2e_chunk, R), dtype=torch.float64).pin_memory()
+    wav = [torch.empty(e2e_chunk, dtype=torch.float64).pin_memory() for _ in ws]
+    outs = [(torch.empty((x.shots, e2e_chunk, x.rec.shape[0]), dtype=torch.float64).pin_memory(),
+             torch.empty((x.shots, e2e_chunk, x.rec.shape[0]), dtype=torch.float64).pin_memory()) for x in ws]
     barrier(dist, device)
     t0 = time.perf_counter()
     for c in range(e2e_steps // e2e_chunk):
         t_at = W_steps + c * e2e_chunk
-        wav.copy_(torch.from_numpy(s.arrays["wavelet"][t_at:t_at + e2e_chunk]))
-        e.set_wavelet(t_at, wav)
+        for k, s in enumerate(setups):
+            wav[k].copy_(torch.from_numpy(s.arrays["wavelet"][t_at:t_at + e2e_chunk]))
+            e.set_wavelet(t_at, wav[k], mesh=k)
         e.step(e2e_chunk)
-        e.fetch_traces(t_at, e2e_chunk, out_x=out_x, out_z=out_z)
+        for k in range(len(ws)):
+            e.fetch_traces(t_at, e2e_chunk, mesh=k, out_x=outs[k][0], out_z=outs[k][1])
     t_e2e = time.perf_counter() - t0
     barrier(dist, device)
     t_e2e = max_over_ranks(t_e2e, dist, device)
     e2e_value = world * dof_step * e2e_steps / t_e2e
-    h2d = 8.0  # one wavelet sample per step
-    d2h = 2.0 * S * R * 8.0
+    h2d = 8.0 * len(ws)
+    d2h = 2.0 * 8.0 * R_tot
 
-    # ---- accuracy: FP32 batch against FP64 batch over the first steps -----------------------
+    # ---- accuracy: the batch against FP64 over the first steps -----------------------------
+    def traces(engine):
+        out = []
+        for k, x in enumerate(ws):
+            for m in range(x.shots):
+                out += [engine.fetch("trace_x", k, m).ravel(), engine.fetch("trace_z", k, m).ravel()]
+        return np.concatenate(out)
+
     e.reset()
     e.step(acc_steps)
-    tr32 = [e.fetch("trace_x", 0, m) for m in range(S)] + [e.fetch("trace_z", 0, m) for m in range(S)]
+    tr = traces(e)
     e.close()
-    with eng.Engine(mesh, "fp64", device=device) as e64:
-        e64.step(acc_steps)
-        tr64 = [e64.fetch("trace_x", 0, m) for m in range(S)] + [e64.fetch("trace_z", 0, m) for m in range(S)]
-    a32, a64 = np.concatenate([x.ravel() for x in tr32]), np.concatenate([x.ravel() for x in tr64])
-    trace_err = float(np.linalg.norm(a32 - a64) / max(np.linalg.norm(a64), 1e-300))
+    accuracy = None
+    if args.precision != "fp64":
+        with eng.Engine(meshes, "fp64", device=device) as e64:
+            e64.step(acc_steps)
+            tr64 = traces(e64)
+        accuracy = {"trace_rel_l2_vs_fp64": float(np.linalg.norm(tr - tr64) / max(np.linalg.norm(tr64), 1e-300)),
+                    "steps": acc_steps, "shots": S_tot}
 
-    # ---- plain FP64 path on the same mesh: one shot, L2 flushed before every step -----------
-    w1 = P.workloads.Workload(w.name, w.mesh, w.vp, w.vs, w.rho, w.fp, w.sponge, w.src[:1], w.rec, w.steps)
-    s1 = P.host.build_setup(w1, full=False, n_steps=table)
+    # ---- plain FP64 path on the first mesh: one shot, L2 flushed before every step ----------
+    s1 = P.host.build_setup(one_shot(ws[0]), full=False, n_steps=table)
     with eng.Engine(eng.mesh_from_setup(s1, with_ref_ops=False), "fp64", device=device) as e1:
         e1.step(W_steps)
-        mv1, ms1, tot1 = e1.step_profiled(K_steps, flush_l2=True)
-        fp64_value = e1.stats()["dof_per_step"] * K_steps / (tot1 * 1e-3)
-        fp64_bytes = e1.stats()["bytes_per_step"]
+        _, _, tot1 = e1.step_profiled(K_steps, flush_l2=True)
+        st1 = e1.stats()
+    fp64_value = st1["dof_per_step"] * K_steps / (tot1 * 1e-3)
     clocks = sampler.stop()
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K_steps, "warmup": W_steps,
             "ms_per_step": t_max / K_steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded jittered-grid mesh, layered medium)",
-            "config": {"workload": desc, "K": Kel, "shots": S, "receivers": R, "precision": "fp32",
-                       "parallelism": "independent shot batches per GPU" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2: state %.2f GB per GPU" % (30 * S * Kel * 4 / 1e9),
+            "dtype": {"fp32": "f32", "fp32_kahan": "f32 (Kahan-compensated)", "fp64": "f64"}[args.precision],
+            "data": "synthetic (seeded meshes and media)",
+            "config": {"workload": desc, "meshes": len(ws), "K": K_tot, "shots": S_tot, "precision": args.precision,
+                       "kernels": eng.KERNEL_FAMILIES[st["kernel_family"]],
+                       "parallelism": "independent batches per GPU" if world > 1 else "single GPU",
+                       "l2": ("inputs larger than L2: state %.2f GB per GPU" % (state_bytes / 1e9))
+                       if state_bytes > 126e6 * 1.5 else "state smaller than L2 (not flushed)",
                        "block_threads": st["block_threads"]},
             "gpu_launches": 2 * K_steps,
             "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "bytes_per_launch": dom[1], "ms_per_launch": dom[2],
                          "step_GBs": bytes_step / (t_max / K_steps * 1e-3) / 1e9,
-                         "kernels": {"k_velocity": {"ms": t_vel, "GBs": b_vel / (t_vel * 1e-3) / 1e9},
-                                     "k_stress": {"ms": t_str, "GBs": b_str / (t_str * 1e-3) / 1e9}}},
-            "fp64_plain": {"value": fp64_value, "unit": UNIT, "shots": 1, "l2": "flushed before every step",
-                           "ms_per_step": tot1 / K_steps,
-                           "GBs": fp64_bytes / (tot1 / K_steps * 1e-3) / 1e9,
-                           "ratio_fp32_batched_over_fp64_plain": value / world / fp64_value},
-            "accuracy": {"trace_rel_l2_fp32_vs_fp64": trace_err, "steps": acc_steps, "shots": S},
+                         "kernels": {names[0]: {"ms": t_vel, "GBs": b_vel / (t_vel * 1e-3) / 1e9},
+                                     names[1]: {"ms": t_str, "GBs": b_str / (t_str * 1e-3) / 1e9}}},
+            "fp64_plain": {"value": fp64_value, "unit": UNIT, "shots": 1, "K": ws[0].K,
+                           "l2": "flushed before every step", "ms_per_step": tot1 / K_steps,
+                           "GBs": st1["bytes_per_step"] / (tot1 / K_steps * 1e-3) / 1e9,
+                           "ratio_batched_over_fp64_plain": value / world / fp64_value},
+            "accuracy": accuracy,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "chunk_steps": e2e_chunk,
                     "what": "dg_gpu_set_wavelet (pinned host wavelet) + dg_gpu_step + dg_gpu_fetch_traces "
                             "(all shots, pinned host buffers) per %d-step chunk, wall clock" % e2e_chunk},
             "clocks": clocks}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_reference(w)
+        line["cpu_baseline"] = cpu_reference(ws[0])
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -376,6 +416,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="multishot")
+    ap.add_argument("--precision", choices=["fp32", "fp32_kahan", "fp64"], default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     if args.warmup < 3:

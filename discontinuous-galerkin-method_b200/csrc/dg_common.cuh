@@ -1,0 +1,116 @@
+// dg_common.cuh — shared definitions of the sm_100a kernels of the DG elastic-wave time loop (P2, Np = 6, Nfp = 3).
+//
+// Data layout in HBM (one mesh):
+//   state   U[plane][g], plane = 6*field + node (fields Vx, Vz, Txx, Tzz, Txz), g = e*S + s
+//           (element e in locality order, shot s innermost); plane stride P = Kp*S.
+//   geo     R4[Kp]  rx, sx, rz, sz (inverse Jacobian, as fun_DG.c:1162-1165)
+//   mat     R4[Kp]  1/rho, lambda, mu, lambda + 2 mu (the distinct entries of A/B, fun_DG.c:1076-1086)
+//   face    int4[Kp] three face codes and a flag word (see face_code below)
+//   sponge  R[6][Kp] absorb_fun, read only for elements whose flag says they are in the sponge
+// One thread advances one (element, shot) pair; a warp therefore reads every state plane as a
+// contiguous run of 32 values, and for S >= 32 a neighbour gather is a contiguous run as well.
+//
+// Face code: -1 on the outer boundary (exterior state 0, Edge_flag = 0, fun_DG.c:720-738),
+// else nb << 4 | nb_in_sponge << 3 | nb_face << 1 | flip, where nb is the neighbour element,
+// nb_face its face that touches ours and flip says its face nodes run the other way
+// (NeighborNodes, fun_DG.c:1195-1276).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dg {
+
+constexpr int NP = 6;
+constexpr int NF = 3;
+constexpr int NPLANES = 30;
+
+// P2 face nodes, 0-based, face j position k (IBE for N = 2, fun_DG.c:1046-1057):
+// {5,3,0}, {0,1,2}, {5,4,2}, packed as nibbles so a runtime (face, k) needs no memory.
+constexpr unsigned long long FACE_NODES = 0x245210035ULL;
+__host__ __device__ __forceinline__ int face_node(int j, int k) {
+  return (int)((FACE_NODES >> (4 * (3 * j + k))) & 15ULL);
+}
+
+template <class R> struct R4T;
+template <> struct R4T<float> { using type = float4; };
+template <> struct R4T<double> { using type = double4; };
+
+// Constant operators, passed by value as kernel parameters so every FMA reads them straight
+// from the parameter bank.  L[j][i][k] is the face-j lift (S_j of the reference).
+template <class R> struct Ops {
+  R Dr[NP * NP];
+  R Ds[NP * NP];
+  R L[NF * NP * NF];
+  R M[NP * NP];  // reference mass matrix inv(V V^T), energy only
+};
+
+template <class R> struct MeshDev {
+  long long P;            // plane stride of the plane-major layout (Kp * S)
+  long long ES, PS;       // value (e, plane, s) lives at U[e*ES + plane*PS + s] in either layout
+  long long steps;        // this mesh's wavelet length
+  int K, Kp, S, n_rec;
+  int n_elem_blocks;      // element blocks of this mesh (grid = these + recorder blocks)
+  int sponge_elems;
+  R dt;
+  R* U;                   // [30][P]
+  R* C;                   // Kahan compensation [30][P] (FP32_KAHAN) or null
+  const typename R4T<R>::type* geo;
+  const typename R4T<R>::type* mat;
+  const int4* face;
+  const R* sponge;        // [6][Kp]
+  const double* wavelet;  // [steps]
+  const int* src_elem;    // [S]
+  const R* src_fun;       // [S][6]
+  const int* rec_elem;    // [n_rec]
+  const int* rec_node;    // [n_rec]
+  R* trace;               // [steps][2][n_rec][S]
+  // reference-operator (bit-exact) path
+  const double* Dx;       // [36][Kp]
+  const double* Dz;       // [36][Kp]
+  const double* Q;        // [30][Kp]
+  const double* AB;       // [10][Kp]: A0..A4, B0..B4
+};
+
+// step counters: ctr[0] is read by the velocity kernel, ctr[1] by the stress kernel.  Each
+// kernel writes only the counter the other one reads, so a captured graph can be replayed.
+struct Counters { long long v, s; };
+
+template <class R> __device__ __forceinline__ R ldg(const R* p) { return __ldg(p); }
+__device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ld4(const double4* p) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// -------------------------------------------------------------------------------------------
+// block -> (mesh, local block) for batches of several meshes
+struct BlockMap { int mesh; int local; };
+
+template <bool MULTI, class R>
+__device__ __forceinline__ const MeshDev<R>* pick_mesh(const MeshDev<R>& one, const MeshDev<R>* tab,
+                                                        const int2* btab, int& local) {
+  if (!MULTI) { local = blockIdx.x; return &one; }
+  const int2 b = __ldg(btab + blockIdx.x);
+  local = b.y;
+  return tab + b.x;
+}
+
+
+// Receiver gather of the reference's Record (OpenMP_Function.c:61-72, stride 2): thread q of
+// the recorder blocks copies V at (receiver element, node) for one (receiver, shot).
+template <class R>
+__device__ __forceinline__ void record(const MeshDev<R>& m, int lb_rec, long long t) {
+  const int q = lb_rec * blockDim.x + threadIdx.x;
+  const int S = m.S;
+  if (q >= m.n_rec * S) return;
+  const int r = q / S, s = q - r * S;
+  const int e = __ldg(m.rec_elem + r), node = __ldg(m.rec_node + r);
+  const long long at = (long long)e * m.ES + s;
+  R* tr = m.trace + (t * 2) * (long long)m.n_rec * S;
+  tr[q] = m.U[at + (0 + node) * m.PS];
+  tr[(long long)m.n_rec * S + q] = m.U[at + (6 + node) * m.PS];
+}
+
+
+}  // namespace dg

@@ -6,7 +6,11 @@
 // and uploads everything.  dg_gpu_step replays a CUDA graph of `graph_steps` steps, each step
 // being one velocity and one stress launch (the stress launch also records the receivers).
 #include "dg_gpu.h"
-#include "dg_kernels.cuh"
+#include "dg_aux.cuh"
+#include "dg_common.cuh"
+#include "dg_step_generic.cuh"
+#include "dg_step_ref.cuh"
+#include "dg_step_x2.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -99,7 +103,9 @@ struct dg_gpu_ctx {
   Ops<double> ops_d{};
   Ops<float> ops_f{};
   Ops2 ops2{};
-  int x2 = 0;  // shot count of the two-shot FP32 kernels in use (element-major layout), 0: none
+  // packed FP32x2 kernels in use: 0 none; 1 two elements per thread (one shot, plane-major
+  // layout); S >= 2 two shots per thread (element-major layout U[e][plane][S])
+  int x2 = 0;
   int block = 256;
   int blocks_v = 0, blocks_t = 0;
   bool multi = false;
@@ -323,7 +329,7 @@ int upload_mesh(dg_gpu_ctx* c, const dg_gpu_mesh& m, Prepared& p, MeshDev<R>& d)
   d.S = p.S;
   d.n_rec = p.n_rec;
   d.P = (long long)p.Kp * p.S;
-  if (c->x2) {  // element-major: U[e][plane][S]
+  if (c->x2 >= 2) {  // element-major: U[e][plane][S]
     d.ES = 30LL * p.S;
     d.PS = p.S;
   } else {      // plane-major: U[plane][e*S + s]
@@ -415,7 +421,7 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
   std::vector<int2> bv, bt;
   for (size_t k = 0; k < md.size(); k++) {
     MeshHostInfo& h = c->mi[k];
-    const long long lanes = c->x2 ? (long long)h.K * (h.S / 2) : (long long)h.K * h.S;
+    const long long lanes = c->x2 == 1 ? h.Kp / 2 : (c->x2 ? (long long)h.K * (h.S / 2) : (long long)h.K * h.S);
     h.elem_blocks = (int)((lanes + B - 1) / B);
     h.rec_blocks = (h.n_rec * h.S + B - 1) / B;
     md[k].n_elem_blocks = h.elem_blocks;
@@ -447,6 +453,11 @@ int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid) {
   const dim3 bl(c->block), gv(c->blocks_v), gt(c->blocks_t);
   cudaStream_t st = c->stream;
   switch (c->x2) {
+    case 1:  // one shot: two elements per thread
+      k_velocity_x2e<KAHAN><<<gv, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress_x2e<KAHAN><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);
+      break;
 #define DG_X2(SS)                                                                      \
   case SS:                                                                             \
     k_velocity_x2<SS, KAHAN><<<gv, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);       \
@@ -669,9 +680,9 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   {
     const int S0 = meshes[0].n_shots;
     const bool fits = (long long)meshes[0].K * (S0 / 2) < (1LL << 31);
-    if (!c->multi && !c->is_double && o.variant != 1 && x2_supported(S0) && fits) c->x2 = S0;
+    if (!c->multi && !c->is_double && o.variant != 1 && (S0 == 1 || x2_supported(S0)) && fits) c->x2 = S0;
     if (o.variant == 2 && !c->x2)
-      return fail(DG_ERR_UNSUPPORTED, "the two-shot kernels need one FP32 mesh with 2, 4, ..., 128 shots");
+      return fail(DG_ERR_UNSUPPORTED, "the packed kernels need one FP32 mesh with 1, 2, 4, ..., 128 shots");
   }
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   for (auto& e : c->ev) CK(cudaEventCreate(&e));
@@ -977,6 +988,7 @@ int dg_gpu_stats_get(dg_gpu_ctx* c, dg_gpu_stats* out) {
   c->stats.steps_done = c->t;
   c->stats.block_threads = c->block;
   c->stats.graph_steps = c->graph_steps;
+  c->stats.kernel_family = c->precision == DG_FP64_REF ? 0 : (c->x2 == 1 ? 3 : (c->x2 ? 2 : 1));
   *out = c->stats;
   return DG_OK;
 }

@@ -75,7 +75,14 @@ class _Opts(C.Structure):
 class _Stats(C.Structure):
     _fields_ = [("ms_velocity", C.c_double), ("ms_stress", C.c_double), ("launches", C.c_long),
                 ("steps_done", C.c_long), ("block_threads", C.c_int), ("graph_steps", C.c_int),
-                ("bytes_per_step", C.c_double), ("dof_per_step", C.c_double)]
+                ("bytes_per_step", C.c_double), ("dof_per_step", C.c_double), ("kernel_family", C.c_int)]
+
+KERNEL_FAMILIES = {0: "reference operators (k_velocity_ref/k_stress_ref)",
+                   1: "one (element, shot) per thread (k_velocity/k_stress)",
+                   2: "two shots per thread, packed FP32x2 (k_velocity_x2/k_stress_x2)",
+                   3: "two elements per thread, packed FP32x2 (k_velocity_x2e/k_stress_x2e)"}
+KERNEL_NAMES = {0: ("k_velocity_ref", "k_stress_ref"), 1: ("k_velocity", "k_stress"),
+                2: ("k_velocity_x2", "k_stress_x2"), 3: ("k_velocity_x2e", "k_stress_x2e")}
 
 
 _LIB = None

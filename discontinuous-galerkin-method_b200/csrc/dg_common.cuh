@@ -50,6 +50,8 @@ template <class R> struct MeshDev {
   long long steps;        // this mesh's wavelet length
   int K, Kp, S, n_rec;
   int n_elem_blocks;      // element blocks of this mesh (grid = these + recorder blocks)
+  int kind;               // FP32 kernel body: 0 one (element, shot) per thread, plane-major;
+                          // 1 two elements per thread (S = 1); 2 two shots per thread, element-major
   int sponge_elems;
   R dt;
   R* U;                   // [30][P]

@@ -9,6 +9,7 @@
 #include "dg_aux.cuh"
 #include "dg_common.cuh"
 #include "dg_step_generic.cuh"
+#include "dg_step_multi.cuh"
 #include "dg_step_ref.cuh"
 #include "dg_step_x2.cuh"
 
@@ -71,6 +72,8 @@ void set_last_error(const char* msg) { g_last = msg ? msg : ""; }
 struct MeshHostInfo {
   long K = 0;
   int Kp = 0, S = 0, n_rec = 0;
+  int S_pad = 0;  // shots stored (S plus a silent shot where the packed kernels need an even count)
+  int kind = 0;   // kernel body (MeshDev::kind)
   long steps = 0;
   std::vector<int> new_of_old;  // caller element -> internal element
   int* d_new_of_old = nullptr;
@@ -106,6 +109,7 @@ struct dg_gpu_ctx {
   // packed FP32x2 kernels in use: 0 none; 1 two elements per thread (one shot, plane-major
   // layout); S >= 2 two shots per thread (element-major layout U[e][plane][S])
   int x2 = 0;
+  bool mx = false;  // FP32 batch of meshes: per-block dispatch to the packed bodies (k_*_mx)
   int block = 256;
   int blocks_v = 0, blocks_t = 0;
   bool multi = false;
@@ -149,6 +153,8 @@ constexpr long long P2_IBE[9] = {6, 4, 1, 1, 2, 3, 6, 5, 3};
 struct Prepared {
   long K;
   int Kp, S, n_rec;
+  int S_pad = 0;  // shots stored and computed (S, or S + 1 silent shot for the packed kernels)
+  int kind = 0;   // kernel body, as MeshDev::kind
   std::vector<int> order;       // internal -> caller element
   std::vector<int> new_of_old;  // caller -> internal
   std::vector<double> geo;      // [Kp][4] rx sx rz sz
@@ -280,8 +286,9 @@ int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
       for (int i = 0; i < 6; i++) p.sponge[(size_t)i * Kp + n] = m.absorb_fun[e * 6 + i];
     }
   }
-  p.src_elem.resize(p.S);
-  p.src_fun.resize((size_t)p.S * 6);
+  // padded (silent) shots: no source element, zero source vector
+  p.src_elem.assign(p.S_pad, -1);
+  p.src_fun.assign((size_t)p.S_pad * 6, 0.0);
   for (int s = 0; s < p.S; s++) {
     const long tri = m.source[s * 2 + 0] - 1, node = m.source[s * 2 + 1] - 1;
     if (tri < 0 || tri >= K || node < 0 || node >= 6) return fail(DG_ERR_MESH, "source out of range");
@@ -326,14 +333,15 @@ int upload_mesh(dg_gpu_ctx* c, const dg_gpu_mesh& m, Prepared& p, MeshDev<R>& d)
   memset(&d, 0, sizeof d);
   d.K = (int)p.K;
   d.Kp = p.Kp;
-  d.S = p.S;
+  d.S = p.S_pad;
   d.n_rec = p.n_rec;
-  d.P = (long long)p.Kp * p.S;
-  if (c->x2 >= 2) {  // element-major: U[e][plane][S]
-    d.ES = 30LL * p.S;
-    d.PS = p.S;
-  } else {      // plane-major: U[plane][e*S + s]
-    d.ES = p.S;
+  d.kind = p.kind;
+  d.P = (long long)p.Kp * p.S_pad;
+  if (p.kind == 2) {  // element-major: U[e][plane][S]
+    d.ES = 30LL * p.S_pad;
+    d.PS = p.S_pad;
+  } else {            // plane-major: U[plane][e*S + s]
+    d.ES = p.S_pad;
     d.PS = d.P;
   }
   d.steps = m.n_steps;
@@ -376,7 +384,7 @@ int upload_mesh(dg_gpu_ctx* c, const dg_gpu_mesh& m, Prepared& p, MeshDev<R>& d)
   if ((rc = c->upload(&rn, p.rec_node))) return rc;
   d.rec_elem = re;
   d.rec_node = rn;
-  const size_t trace_elems = (size_t)m.n_steps * 2 * std::max(1, p.n_rec) * p.S;
+  const size_t trace_elems = (size_t)m.n_steps * 2 * std::max(1, p.n_rec) * p.S_pad;
   if ((rc = c->alloc(&d.trace, trace_elems))) return rc;
   CK(cudaMemsetAsync(d.trace, 0, sizeof(R) * trace_elems, c->stream));
   if (c->precision == DG_FP64_REF) {
@@ -421,9 +429,10 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
   std::vector<int2> bv, bt;
   for (size_t k = 0; k < md.size(); k++) {
     MeshHostInfo& h = c->mi[k];
-    const long long lanes = c->x2 == 1 ? h.Kp / 2 : (c->x2 ? (long long)h.K * (h.S / 2) : (long long)h.K * h.S);
+    const long long lanes =
+        h.kind == 1 ? h.Kp / 2 : (h.kind == 2 ? (long long)h.K * (h.S_pad / 2) : (long long)h.K * h.S_pad);
     h.elem_blocks = (int)((lanes + B - 1) / B);
-    h.rec_blocks = (h.n_rec * h.S + B - 1) / B;
+    h.rec_blocks = (h.n_rec * h.S_pad + B - 1) / B;
     md[k].n_elem_blocks = h.elem_blocks;
     for (int b = 0; b < h.elem_blocks; b++) bv.push_back(make_int2((int)k, b));
     for (int b = 0; b < h.elem_blocks + h.rec_blocks; b++) bt.push_back(make_int2((int)k, b));
@@ -446,7 +455,25 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
 }
 
 // shot counts with a two-shot FP32 kernel instance
-bool x2_supported(int S) { return S == 2 || S == 4 || S == 8 || S == 16 || S == 32 || S == 64 || S == 128; }
+bool x2_supported(int S) { return (S >= 2 && S <= 16 && S % 2 == 0) || S == 32 || S == 64 || S == 128; }
+
+// Kernel body and stored shot count for a mesh of S shots: FP32 meshes use the packed bodies —
+// two elements per thread for one shot, two shots per thread otherwise, an odd count padded with
+// one silent shot — unless the caller asks for one (element, shot) per thread (variant 1).
+void choose_kind(int S, long K, bool fp32, int variant, int& kind, int& S_pad) {
+  kind = 0;
+  S_pad = S;
+  if (!fp32 || variant == 1) return;
+  if (S == 1) {
+    kind = 1;
+    return;
+  }
+  const int even = S + (S & 1);
+  if (x2_supported(even) && (long long)K * (even / 2) < (1LL << 31)) {
+    kind = 2;
+    S_pad = even;
+  }
+}
 
 template <bool KAHAN>
 int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid) {
@@ -464,7 +491,7 @@ int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid) {
     if (mid) CK(cudaEventRecord(mid, st));                                             \
     k_stress_x2<SS, KAHAN><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);         \
     break;
-    DG_X2(2) DG_X2(4) DG_X2(8) DG_X2(16) DG_X2(32) DG_X2(64) DG_X2(128)
+    DG_X2(2) DG_X2(4) DG_X2(6) DG_X2(8) DG_X2(10) DG_X2(12) DG_X2(14) DG_X2(16) DG_X2(32) DG_X2(64) DG_X2(128)
 #undef DG_X2
     default:
       return fail(DG_ERR_UNSUPPORTED, "no two-shot kernel for this shot count");
@@ -496,6 +523,16 @@ int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid =
       k_velocity<double, false, false><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
       k_stress<double, false, false><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
+    }
+  } else if (c->mx) {
+    if (c->kahan) {
+      k_velocity_mx<true><<<gv, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress_mx<true><<<gt, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_t, c->d_ctr);
+    } else {
+      k_velocity_mx<false><<<gv, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
+      if (mid) CK(cudaEventRecord(mid, st));
+      k_stress_mx<false><<<gt, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_t, c->d_ctr);
     }
   } else if (c->x2) {
     int rc = c->kahan ? launch_x2<true>(c, mid) : launch_x2<false>(c, mid);
@@ -561,10 +598,10 @@ int zero_state(dg_gpu_ctx* c) {
     void* U = c->is_double ? (void*)c->md_d[k].U : (void*)c->md_f[k].U;
     void* C = c->is_double ? (void*)c->md_d[k].C : (void*)c->md_f[k].C;
     void* T = c->is_double ? (void*)c->md_d[k].trace : (void*)c->md_f[k].trace;
-    const size_t P = (size_t)h.Kp * h.S;
+    const size_t P = (size_t)h.Kp * h.S_pad;
     CK(cudaMemsetAsync(U, 0, esz * NPLANES * P, c->stream));
     if (C) CK(cudaMemsetAsync(C, 0, esz * NPLANES * P, c->stream));
-    CK(cudaMemsetAsync(T, 0, esz * (size_t)h.steps * 2 * std::max(1, h.n_rec) * h.S, c->stream));
+    CK(cudaMemsetAsync(T, 0, esz * (size_t)h.steps * 2 * std::max(1, h.n_rec) * h.S_pad, c->stream));
   }
   CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -677,13 +714,7 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   c->kahan = o.precision == DG_FP32_KAHAN;
   c->multi = n_meshes > 1;
   c->watchdog_every = std::max(0, o.watchdog_every);
-  {
-    const int S0 = meshes[0].n_shots;
-    const bool fits = (long long)meshes[0].K * (S0 / 2) < (1LL << 31);
-    if (!c->multi && !c->is_double && o.variant != 1 && (S0 == 1 || x2_supported(S0)) && fits) c->x2 = S0;
-    if (o.variant == 2 && !c->x2)
-      return fail(DG_ERR_UNSUPPORTED, "the packed kernels need one FP32 mesh with 1, 2, 4, ..., 128 shots");
-  }
+  c->mx = c->multi && !c->is_double;
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   for (auto& e : c->ev) CK(cudaEventCreate(&e));
 
@@ -693,12 +724,18 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   const size_t w = c->is_double ? 8 : 4;
   for (int k = 0; k < n_meshes; k++) {
     Prepared p;
+    choose_kind(meshes[k].n_shots, meshes[k].K, !c->is_double, o.variant, p.kind, p.S_pad);
+    if (o.variant == 2 && p.kind == 0)
+      return fail(DG_ERR_UNSUPPORTED, "no packed FP32 kernel for this mesh (FP32 only; at most 128 shots)");
     int rc = prepare(meshes[k], o.precision, o.reorder, p);
     if (rc) return rc;
     MeshHostInfo& h = c->mi[k];
     h.K = p.K;
     h.Kp = p.Kp;
     h.S = p.S;
+    h.S_pad = p.S_pad;
+    h.kind = p.kind;
+    if (!c->multi) c->x2 = p.kind == 1 ? 1 : (p.kind == 2 ? p.S_pad : 0);
     h.n_rec = p.n_rec;
     h.steps = meshes[k].n_steps;
     h.dt = meshes[k].dt;
@@ -791,7 +828,7 @@ static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
     if (c->watchdog_every > 0 && c->t % c->watchdog_every == 0) {
       CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
       for (size_t k = 0; k < c->mi.size(); k++) {
-        const long long nvals = 30LL * c->mi[k].Kp * c->mi[k].S;
+        const long long nvals = 30LL * c->mi[k].Kp * c->mi[k].S_pad;
         if (c->is_double) k_nonfinite<double><<<592, 256, 0, c->stream>>>(c->md_d[k].U, nvals, c->d_flag);
         else k_nonfinite<float><<<592, 256, 0, c->stream>>>(c->md_f[k].U, nvals, c->d_flag);
         c->stats.launches++;
@@ -883,9 +920,9 @@ int dg_gpu_fetch_traces(dg_gpu_ctx* c, int mesh, long t0, long n, double* dst_x,
   const int B = 256;
   const int grid = (int)((2 * per + B - 1) / B);
   if (c->is_double)
-    k_fetch_traces<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].trace, h.n_rec, h.S, t0, n, c->d_stage);
+    k_fetch_traces<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].trace, h.n_rec, h.S_pad, h.S, t0, n, c->d_stage);
   else
-    k_fetch_traces<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].trace, h.n_rec, h.S, t0, n, c->d_stage);
+    k_fetch_traces<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].trace, h.n_rec, h.S_pad, h.S, t0, n, c->d_stage);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(dst_x, c->d_stage, per * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(dst_z, c->d_stage + per, per * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -917,9 +954,11 @@ int dg_gpu_fetch(dg_gpu_ctx* c, int what, int mesh, int shot, double* dst) {
       const int grid = (int)((n + B - 1) / B);
       const int comp = what - DG_TRACE_X;
       if (c->is_double)
-        k_fetch_trace<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].trace, comp, h.n_rec, h.S, shot, steps, c->d_stage);
+        k_fetch_trace<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].trace, comp, h.n_rec, h.S_pad, shot, steps,
+                                                         c->d_stage);
       else
-        k_fetch_trace<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].trace, comp, h.n_rec, h.S, shot, steps, c->d_stage);
+        k_fetch_trace<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].trace, comp, h.n_rec, h.S_pad, shot, steps,
+                                                        c->d_stage);
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(dst, c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     }
@@ -988,7 +1027,8 @@ int dg_gpu_stats_get(dg_gpu_ctx* c, dg_gpu_stats* out) {
   c->stats.steps_done = c->t;
   c->stats.block_threads = c->block;
   c->stats.graph_steps = c->graph_steps;
-  c->stats.kernel_family = c->precision == DG_FP64_REF ? 0 : (c->x2 == 1 ? 3 : (c->x2 ? 2 : 1));
+  c->stats.kernel_family =
+      c->precision == DG_FP64_REF ? 0 : (c->mx ? 4 : (c->x2 == 1 ? 3 : (c->x2 ? 2 : 1)));
   *out = c->stats;
   return DG_OK;
 }

@@ -159,17 +159,8 @@ __device__ __forceinline__ void velocity_rhs_both(const Ops<R>& ops, const MeshD
 
 // Velocity half-step: for its own element the sponge on the five fields and the source on Vz
 // (OpenMP_Function.c:25-58), then V += dt L_V(T) (OpenMP_Function.c:75-185), L_V = (1/rho) h.
-template <class R, bool KAHAN, bool MULTI>
-__global__ void __launch_bounds__(256, 2) k_velocity(const __grid_constant__ Ops<R> ops,
-                                                     const __grid_constant__ MeshDev<R> one,
-                                                     const MeshDev<R>* __restrict__ tab,
-                                                     const int2* __restrict__ btab,
-                                                     Counters* __restrict__ ctr) {
-  int lb;
-  const MeshDev<R>& m = *pick_mesh<MULTI>(one, tab, btab, lb);
-  const long long t = ctr->v;
-  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
-  if (t >= m.steps) return;
+template <class R, bool KAHAN>
+__device__ __forceinline__ void velocity_body(const Ops<R>& ops, const MeshDev<R>& m, int lb, long long t) {
   const int S = m.S;
   const long long g = (long long)lb * blockDim.x + threadIdx.x;
   if (g >= (long long)m.K * S) return;
@@ -253,23 +244,27 @@ __global__ void __launch_bounds__(256, 2) k_velocity(const __grid_constant__ Ops
   }
 }
 
+template <class R, bool KAHAN, bool MULTI>
+__global__ void __launch_bounds__(256, 2) k_velocity(const __grid_constant__ Ops<R> ops,
+                                                     const __grid_constant__ MeshDev<R> one,
+                                                     const MeshDev<R>* __restrict__ tab,
+                                                     const int2* __restrict__ btab,
+                                                     Counters* __restrict__ ctr) {
+  int lb;
+  const MeshDev<R>& m = *pick_mesh<MULTI>(one, tab, btab, lb);
+  const long long t = ctr->v;
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
+  if (t >= m.steps) return;
+  velocity_body<R, KAHAN>(ops, m, lb, t);
+}
+
 // Stress half-step: T = a T + dt L_T(V) (OpenMP_Function.c:188-306),
 //   Txx += dt [ (l+2m) (dxVx + sum_j S_j nx_j dVx) + l (dzVz + sum_j S_j nz_j dVz) ]
 //   Tzz += dt [ l (dxVx + ...) + (l+2m) (dzVz + ...) ]
 //   Txz += dt m [ dxVz + dzVx + sum_j S_j (nz_j dVx + nx_j dVz) ]
 // The trailing blocks of the grid record the receivers (V is final during this kernel).
-template <class R, bool KAHAN, bool MULTI>
-__global__ void __launch_bounds__(256, 2) k_stress(const __grid_constant__ Ops<R> ops,
-                                                   const __grid_constant__ MeshDev<R> one,
-                                                   const MeshDev<R>* __restrict__ tab,
-                                                   const int2* __restrict__ btab,
-                                                   Counters* __restrict__ ctr) {
-  int lb;
-  const MeshDev<R>& m = *pick_mesh<MULTI>(one, tab, btab, lb);
-  const long long t = ctr->s;
-  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
-  if (t >= m.steps) return;
-  if (lb >= m.n_elem_blocks) { record(m, lb - m.n_elem_blocks, t); return; }
+template <class R, bool KAHAN>
+__device__ __forceinline__ void stress_body(const Ops<R>& ops, const MeshDev<R>& m, int lb, long long t) {
   const int S = m.S;
   const long long g = (long long)lb * blockDim.x + threadIdx.x;
   if (g >= (long long)m.K * S) return;
@@ -390,6 +385,21 @@ __global__ void __launch_bounds__(256, 2) k_stress(const __grid_constant__ Ops<R
       m.C[(12 + i) * P + g] = cxx[i]; m.C[(18 + i) * P + g] = czz[i]; m.C[(24 + i) * P + g] = cxz[i];
     }
   }
+}
+
+template <class R, bool KAHAN, bool MULTI>
+__global__ void __launch_bounds__(256, 2) k_stress(const __grid_constant__ Ops<R> ops,
+                                                   const __grid_constant__ MeshDev<R> one,
+                                                   const MeshDev<R>* __restrict__ tab,
+                                                   const int2* __restrict__ btab,
+                                                   Counters* __restrict__ ctr) {
+  int lb;
+  const MeshDev<R>& m = *pick_mesh<MULTI>(one, tab, btab, lb);
+  const long long t = ctr->s;
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
+  if (t >= m.steps) return;
+  if (lb >= m.n_elem_blocks) { record(m, lb - m.n_elem_blocks, t); return; }
+  stress_body<R, KAHAN>(ops, m, lb, t);
 }
 
 }  // namespace dg

@@ -32,16 +32,13 @@ __device__ __forceinline__ void kahan2(float2& u, float2& c, float2 d) {
   u = t;
 }
 
+// Bodies take the mesh, the block's index within that mesh and the step; the __global__
+// wrappers below (one mesh) and the multi-mesh dispatchers (dg_step_multi.cuh) call them.
 template <int S, bool KAHAN>
-__global__ void __launch_bounds__(256, 2) k_velocity_x2(const __grid_constant__ Ops2 ops,
-                                                        const __grid_constant__ MeshDev<float> m,
-                                                        Counters* __restrict__ ctr) {
+__device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
   constexpr int H = S / 2;    // float2 lanes per element
   constexpr int ES = 30 * H;  // element stride in float2
-  const long long t = ctr->v;
-  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
-  if (t >= m.steps) return;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = lb * blockDim.x + threadIdx.x;
   if (g >= m.K * H) return;
   const int e = g / H, q = g - e * H;
   float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * ES + q;
@@ -203,16 +200,20 @@ __global__ void __launch_bounds__(256, 2) k_velocity_x2(const __grid_constant__ 
 }
 
 template <int S, bool KAHAN>
-__global__ void __launch_bounds__(256, 2) k_stress_x2(const __grid_constant__ Ops2 ops,
-                                                      const __grid_constant__ MeshDev<float> m,
-                                                      Counters* __restrict__ ctr) {
+__global__ void __launch_bounds__(256, 2) k_velocity_x2(const __grid_constant__ Ops2 ops,
+                                                        const __grid_constant__ MeshDev<float> m,
+                                                        Counters* __restrict__ ctr) {
+  const long long t = ctr->v;
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
+  if (t >= m.steps) return;
+  velocity_x2_body<S, KAHAN>(ops, m, blockIdx.x, t);
+}
+
+template <int S, bool KAHAN>
+__device__ __forceinline__ void stress_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
   constexpr int H = S / 2;
   constexpr int ES = 30 * H;
-  const long long t = ctr->s;
-  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
-  if (t >= m.steps) return;
-  if ((int)blockIdx.x >= m.n_elem_blocks) { record(m, blockIdx.x - m.n_elem_blocks, t); return; }
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = lb * blockDim.x + threadIdx.x;
   if (g >= m.K * H) return;
   const int e = g / H, q = g - e * H;
   float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * ES + q;
@@ -334,6 +335,17 @@ __global__ void __launch_bounds__(256, 2) k_stress_x2(const __grid_constant__ Op
   }
 }
 
+template <int S, bool KAHAN>
+__global__ void __launch_bounds__(256, 2) k_stress_x2(const __grid_constant__ Ops2 ops,
+                                                      const __grid_constant__ MeshDev<float> m,
+                                                      Counters* __restrict__ ctr) {
+  const long long t = ctr->s;
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
+  if (t >= m.steps) return;
+  if ((int)blockIdx.x >= m.n_elem_blocks) { record(m, blockIdx.x - m.n_elem_blocks, t); return; }
+  stress_x2_body<S, KAHAN>(ops, m, blockIdx.x, t);
+}
+
 // -------------------------------------------------------------------------------------------
 // Two-element FP32 kernels for one shot: the plane-major layout U[plane][Kp] read as float2, so
 // thread p advances elements 2p and 2p+1 with packed arithmetic.  Geometry, materials and face
@@ -369,13 +381,8 @@ __device__ __forceinline__ float2 gather_pair(const MeshDev<float>& m, const Fac
 }
 
 template <bool KAHAN>
-__global__ void __launch_bounds__(256, 2) k_velocity_x2e(const __grid_constant__ Ops2 ops,
-                                                         const __grid_constant__ MeshDev<float> m,
-                                                         Counters* __restrict__ ctr) {
-  const long long t = ctr->v;
-  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
-  if (t >= m.steps) return;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void velocity_x2e_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
+  const int p = lb * blockDim.x + threadIdx.x;
   const int H = m.Kp / 2;  // plane stride in float2
   if (p >= H) return;
   const int e0 = 2 * p, e1 = 2 * p + 1;
@@ -501,14 +508,18 @@ __global__ void __launch_bounds__(256, 2) k_velocity_x2e(const __grid_constant__
 }
 
 template <bool KAHAN>
-__global__ void __launch_bounds__(256, 2) k_stress_x2e(const __grid_constant__ Ops2 ops,
-                                                       const __grid_constant__ MeshDev<float> m,
-                                                       Counters* __restrict__ ctr) {
-  const long long t = ctr->s;
-  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
+__global__ void __launch_bounds__(256, 2) k_velocity_x2e(const __grid_constant__ Ops2 ops,
+                                                         const __grid_constant__ MeshDev<float> m,
+                                                         Counters* __restrict__ ctr) {
+  const long long t = ctr->v;
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
   if (t >= m.steps) return;
-  if ((int)blockIdx.x >= m.n_elem_blocks) { record(m, blockIdx.x - m.n_elem_blocks, t); return; }
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  velocity_x2e_body<KAHAN>(ops, m, blockIdx.x, t);
+}
+
+template <bool KAHAN>
+__device__ __forceinline__ void stress_x2e_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
+  const int p = lb * blockDim.x + threadIdx.x;
   const int H = m.Kp / 2;
   if (p >= H) return;
   const int e0 = 2 * p, e1 = 2 * p + 1;
@@ -610,6 +621,17 @@ __global__ void __launch_bounds__(256, 2) k_stress_x2e(const __grid_constant__ O
 #pragma unroll
     for (int i = 0; i < NP; i++) { Cp[(12 + i) * H] = cxx[i]; Cp[(18 + i) * H] = czz[i]; Cp[(24 + i) * H] = cxz[i]; }
   }
+}
+
+template <bool KAHAN>
+__global__ void __launch_bounds__(256, 2) k_stress_x2e(const __grid_constant__ Ops2 ops,
+                                                       const __grid_constant__ MeshDev<float> m,
+                                                       Counters* __restrict__ ctr) {
+  const long long t = ctr->s;
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
+  if (t >= m.steps) return;
+  if ((int)blockIdx.x >= m.n_elem_blocks) { record(m, blockIdx.x - m.n_elem_blocks, t); return; }
+  stress_x2e_body<KAHAN>(ops, m, blockIdx.x, t);
 }
 
 }  // namespace dg

@@ -80,9 +80,11 @@ class _Stats(C.Structure):
 KERNEL_FAMILIES = {0: "reference operators (k_velocity_ref/k_stress_ref)",
                    1: "one (element, shot) per thread (k_velocity/k_stress)",
                    2: "two shots per thread, packed FP32x2 (k_velocity_x2/k_stress_x2)",
-                   3: "two elements per thread, packed FP32x2 (k_velocity_x2e/k_stress_x2e)"}
+                   3: "two elements per thread, packed FP32x2 (k_velocity_x2e/k_stress_x2e)",
+                   4: "batch of meshes, each block on its mesh's packed body (k_velocity_mx/k_stress_mx)"}
 KERNEL_NAMES = {0: ("k_velocity_ref", "k_stress_ref"), 1: ("k_velocity", "k_stress"),
-                2: ("k_velocity_x2", "k_stress_x2"), 3: ("k_velocity_x2e", "k_stress_x2e")}
+                2: ("k_velocity_x2", "k_stress_x2"), 3: ("k_velocity_x2e", "k_stress_x2e"),
+                4: ("k_velocity_mx", "k_stress_mx")}
 
 
 _LIB = None

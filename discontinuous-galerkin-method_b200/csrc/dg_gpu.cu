@@ -11,6 +11,7 @@
 #include "dg_step_generic.cuh"
 #include "dg_step_multi.cuh"
 #include "dg_step_ref.cuh"
+#include "dg_step_wave.cuh"
 #include "dg_step_x2.cuh"
 
 #include <algorithm>
@@ -97,6 +98,7 @@ struct dg_gpu_ctx {
   int2* d_btab_v = nullptr;
   int2* d_btab_t = nullptr;
   Counters* d_ctr = nullptr;
+  double bytes_two_pass = 0, bytes_wave = 0;  // algorithmic bytes per step of the two step forms
   int* d_flag = nullptr;
   double* d_energy = nullptr;
   double* d_stage = nullptr;
@@ -110,6 +112,11 @@ struct dg_gpu_ctx {
   // layout); S >= 2 two shots per thread (element-major layout U[e][plane][S])
   int x2 = 0;
   bool mx = false;  // FP32 batch of meshes: per-block dispatch to the packed bodies (k_*_mx)
+  bool wave = false;  // one launch per step (k_step_wave), RCM order, chunk schedule in wv
+  Wave wv{};
+  std::vector<int4> face_h;    // face codes of mesh 0 (internal numbering), for the chunk schedule
+  std::vector<int> rec_elem_h; // receiver elements of mesh 0 (internal numbering)
+  int num_sms = 148;
   int block = 256;
   int blocks_v = 0, blocks_t = 0;
   bool multi = false;
@@ -168,6 +175,80 @@ struct Prepared {
   long sponge_elems = 0;
 };
 
+// Reverse Cuthill-McKee numbering of the element adjacency graph (faces with Edge_flag = 1):
+// breadth-first from a pseudo-peripheral element of each connected part, neighbours taken in
+// order of increasing degree, the whole sequence reversed.  Keeps every element's neighbours
+// within a narrow band of numbers.
+std::vector<int> rcm_order(const dg_gpu_mesh& m, long K) {
+  auto nbr = [&](long e, int f) -> long {
+    if (m.Edge_flag[e * 3 + f] != 1) return -1;
+    const long n = m.Neighbor[e * 3 + f] - 1;
+    return (n >= 0 && n < K && n != e) ? n : -1;
+  };
+  std::vector<int> deg(K, 0);
+  for (long e = 0; e < K; e++)
+    for (int f = 0; f < 3; f++) deg[e] += nbr(e, f) >= 0;
+  std::vector<int> stamp(K, -1), queue(K);
+  std::vector<char> placed(K, 0);
+  std::vector<int> seq;
+  seq.reserve(K);
+  int pass = 0;
+  auto sorted_nbrs = [&](long e, long out[3]) {
+    int n = 0;
+    for (int f = 0; f < 3; f++) {
+      const long x = nbr(e, f);
+      if (x >= 0) out[n++] = x;
+    }
+    std::sort(out, out + n, [&](long a, long b) { return deg[a] < deg[b] || (deg[a] == deg[b] && a < b); });
+    return n;
+  };
+  for (long s0 = 0; s0 < K; s0++) {
+    if (placed[s0]) continue;
+    // two sweeps to a far element of minimum degree in the last level
+    long start = s0;
+    for (int sweep = 0; sweep < 2; sweep++) {
+      ++pass;
+      int head = 0, tail = 0;
+      queue[tail++] = (int)start;
+      stamp[start] = pass;
+      int level_begin = 0;
+      while (head < tail) {
+        const int level_end = tail;
+        level_begin = head;
+        while (head < level_end) {
+          const long e = queue[head++];
+          long nb[3];
+          const int n = sorted_nbrs(e, nb);
+          for (int q = 0; q < n; q++)
+            if (stamp[nb[q]] != pass) {
+              stamp[nb[q]] = pass;
+              queue[tail++] = (int)nb[q];
+            }
+        }
+      }
+      long best = queue[level_begin];
+      for (int q = level_begin; q < tail; q++)
+        if (deg[queue[q]] < deg[best]) best = queue[q];
+      start = best;
+    }
+    int head = (int)seq.size();
+    seq.push_back((int)start);
+    placed[start] = 1;
+    while (head < (int)seq.size()) {
+      const long e = seq[head++];
+      long nb[3];
+      const int n = sorted_nbrs(e, nb);
+      for (int q = 0; q < n; q++)
+        if (!placed[nb[q]]) {
+          placed[nb[q]] = 1;
+          seq.push_back((int)nb[q]);
+        }
+    }
+  }
+  std::reverse(seq.begin(), seq.end());
+  return seq;
+}
+
 int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
   if (m.K <= 0 || m.K > (1L << 26)) return fail(DG_ERR_ARG, "K must be in [1, 2^26]");
   if (m.Np != 6 || m.Nfp != 3) return fail(DG_ERR_UNSUPPORTED, "only P2 (Np = 6, Nfp = 3) is supported");
@@ -213,10 +294,13 @@ int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
     cz[e] = (Z[0] + Z[1] + Z[2]) / 3.0;
   }
 
-  // locality order
+  // locality order: Hilbert curve of centroids (1), or reverse Cuthill-McKee (2) for the
+  // wavefront step, which needs every element's neighbours close to it in the numbering
   p.order.resize(K);
   for (long e = 0; e < K; e++) p.order[e] = (int)e;
-  if (reorder) {
+  if (reorder == 2) {
+    p.order = rcm_order(m, K);
+  } else if (reorder) {
     double x0 = cx[0], x1 = cx[0], z0 = cz[0], z1 = cz[0];
     for (long e = 0; e < K; e++) {
       x0 = std::min(x0, cx[e]); x1 = std::max(x1, cx[e]);
@@ -454,6 +538,96 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
   return DG_OK;
 }
 
+// Schedule of the wavefront step for the current block size.  A unit is one warp's 32 threads of
+// the element range (thread g works on element g / H, H = shots / 2); the wait list holds, per unit, the
+// distinct units covering one of its elements or a neighbour of one; the lag L (in blocks) covers
+// the unit bandwidth plus a margin of about half the resident warps, so a stress update seldom
+// waits.  Receivers are listed under every unit that covers their element.
+int build_wave(dg_gpu_ctx* c) {
+  const MeshHostInfo& h = c->mi[0];
+  const long H = h.S_pad / 2;
+  if (c->block % 32) return fail(DG_ERR_UNSUPPORTED, "block size not a multiple of 32");
+  const int WPB = c->block / 32;
+  const long NUl = (h.K * H + 31) / 32;
+  if (NUl >= (1L << 30)) return fail(DG_ERR_UNSUPPORTED, "too many warps for the wavefront step");
+  const int NU = (int)NUl, NB = (NU + WPB - 1) / WPB;
+  auto first_unit = [&](long e) { return (int)(e * H / 32); };
+  auto last_unit = [&](long e) { return (int)(((e + 1) * H - 1) / 32); };
+  std::vector<int> nstart(NU + 1, 0), nlist;
+  nlist.reserve((size_t)NU * 6);
+  int Lb = 0, W = 1;
+  std::vector<int> tmp;
+  for (int u = 0; u < NU; u++) {
+    tmp.clear();
+    const long e0 = (long)u * 32 / H, e1 = std::min<long>(h.K - 1, ((long)u * 32 + 31) / H);
+    for (long e = e0; e <= e1; e++) {
+      const int4 f = c->face_h[e];
+      const long els[4] = {e, f.x >= 0 ? f.x >> 4 : -1, f.y >= 0 ? f.y >> 4 : -1, f.z >= 0 ? f.z >> 4 : -1};
+      for (long x : els)
+        if (x >= 0)
+          for (int v = first_unit(x); v <= last_unit(x); v++) tmp.push_back(v);
+    }
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    for (int k : tmp) nlist.push_back(k);
+    nstart[u + 1] = (int)nlist.size();
+    Lb = std::max(Lb, tmp.back() / WPB - u / WPB);
+    W = std::max(W, (int)tmp.size());
+  }
+  if (W > 32) return fail(DG_ERR_UNSUPPORTED, "wavefront wait list longer than a warp");
+  std::vector<int> wait((size_t)NU * W, -1);
+  for (int u = 0; u < NU; u++)
+    std::copy(nlist.begin() + nstart[u], nlist.begin() + nstart[u + 1], wait.begin() + (size_t)u * W);
+  std::vector<int> rstart(NU + 1, 0), rlist;
+  {
+    std::vector<std::vector<int>> per(NU);
+    for (int r = 0; r < h.n_rec; r++) {
+      const long e = c->rec_elem_h[r];
+      for (int v = first_unit(e); v <= last_unit(e); v++) per[v].push_back(r);
+    }
+    for (int u = 0; u < NU; u++) {
+      rstart[u + 1] = rstart[u] + (int)per[u].size();
+      rlist.insert(rlist.end(), per[u].begin(), per[u].end());
+    }
+    if (rlist.empty()) rlist.push_back(0);
+  }
+  int *d_wait, *d_rs, *d_rl;
+  unsigned* d_flag;
+  unsigned long long* d_tk;
+  int* d_err;
+  int rc;
+  if ((rc = c->upload(&d_wait, wait))) return rc;
+  if ((rc = c->upload(&d_rs, rstart))) return rc;
+  if ((rc = c->upload(&d_rl, rlist))) return rc;
+  if ((rc = c->alloc(&d_flag, NU))) return rc;
+  if ((rc = c->alloc(&d_tk, 1))) return rc;
+  if ((rc = c->alloc(&d_err, 1))) return rc;
+  CK(cudaMemsetAsync(d_flag, 0, sizeof(unsigned) * NU, c->stream));
+  CK(cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
+  Wave& w = c->wv;
+  w.NU = NU;
+  w.NB = NB;
+  w.W = W;
+  // margin over the bandwidth, in blocks: about half the warps resident on the GPU, so that the
+  // velocity updates a stress update needs have mostly finished when it starts, while the lag
+  // window stays in L2 (DG_WAVE_MARGIN overrides it, for tuning)
+  int margin = (c->num_sms * 8 + WPB - 1) / WPB;
+  if (const char* env = getenv("DG_WAVE_MARGIN")) margin = std::max(0, atoi(env));
+  w.L = Lb + margin;
+  w.wait = d_wait;
+  w.vflag = d_flag;
+  w.rec_start = d_rs;
+  w.rec_list = d_rl;
+  w.tickets = d_tk;
+  w.error = d_err;
+  w.spin_limit = 1u << 20;  // a million polls of an L2 line: well under a second
+  c->blocks_v = NB + w.L;
+  c->blocks_t = 0;
+  k_wave_sync<<<1, 1, 0, c->stream>>>(c->d_ctr, d_tk, (unsigned)c->blocks_v);
+  CK(cudaGetLastError());
+  return DG_OK;
+}
+
 // shot counts with a two-shot FP32 kernel instance
 bool x2_supported(int S) { return (S >= 2 && S <= 16 && S % 2 == 0) || S == 32 || S == 64 || S == 128; }
 
@@ -499,6 +673,25 @@ int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid) {
   return DG_OK;
 }
 
+// shot counts with a wavefront step instance
+bool wave_supported(int S) { return S == 2 || S == 4 || S == 8 || S == 16 || S == 32 || S == 64 || S == 128; }
+
+template <bool KAHAN>
+int launch_wave(dg_gpu_ctx* c) {
+  const dim3 bl(c->block), g(c->blocks_v);
+  switch (c->x2) {
+#define DG_WV(SS)                                                                           \
+  case SS:                                                                                  \
+    k_step_wave<SS, KAHAN><<<g, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr); \
+    break;
+    DG_WV(2) DG_WV(4) DG_WV(8) DG_WV(16) DG_WV(32) DG_WV(64) DG_WV(128)
+#undef DG_WV
+    default:
+      return fail(DG_ERR_UNSUPPORTED, "no wavefront step for this shot count");
+  }
+  return DG_OK;
+}
+
 int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid = nullptr, cudaEvent_t after = nullptr) {
   const dim3 bl(c->block);
   const dim3 gv(c->blocks_v), gt(c->blocks_t);
@@ -524,6 +717,10 @@ int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid =
       if (mid) CK(cudaEventRecord(mid, st));
       k_stress<double, false, false><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
     }
+  } else if (c->wave) {  // the whole step in one launch: it is timed as the "velocity" interval
+    int rc = c->kahan ? launch_wave<true>(c) : launch_wave<false>(c);
+    if (rc) return rc;
+    if (mid) CK(cudaEventRecord(mid, st));
   } else if (c->mx) {
     if (c->kahan) {
       k_velocity_mx<true><<<gv, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
@@ -587,7 +784,24 @@ int set_block(dg_gpu_ctx* c, int block) {
   c->block = block;
   int rc = c->is_double ? layout(c, c->md_d, &c->d_tab_d) : layout(c, c->md_f, &c->d_tab_f);
   if (rc) return rc;
+  if (c->wave && (rc = build_wave(c))) {
+    if (rc != DG_ERR_UNSUPPORTED) return rc;
+    c->wave = false;  // the two-launch step serves this mesh
+  }
   CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
+// DG_ERR_TIMEOUT if a wavefront wait gave up since the last check (then cleared)
+int check_wave(dg_gpu_ctx* c) {
+  if (!c->wave) return DG_OK;
+  int err = 0;
+  CK(cudaMemcpyAsync(&err, c->wv.error, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (err) {
+    CK(cudaMemsetAsync(c->wv.error, 0, sizeof(int), c->stream));
+    return fail(DG_ERR_TIMEOUT, "a wait between blocks of the wavefront step reached its limit");
+  }
   return DG_OK;
 }
 
@@ -604,6 +818,11 @@ int zero_state(dg_gpu_ctx* c) {
     CK(cudaMemsetAsync(T, 0, esz * (size_t)h.steps * 2 * std::max(1, h.n_rec) * h.S_pad, c->stream));
   }
   CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), c->stream));
+  if (c->wave) {  // step ids restart at 1: clear the published flags and the tickets
+    CK(cudaMemsetAsync(c->wv.vflag, 0, sizeof(unsigned) * c->wv.NU, c->stream));
+    CK(cudaMemsetAsync(c->wv.tickets, 0, sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(c->wv.error, 0, sizeof(int), c->stream));
+  }
   CK(cudaStreamSynchronize(c->stream));
   c->t = 0;
   return DG_OK;
@@ -709,6 +928,7 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
 
   std::unique_ptr<dg_gpu_ctx> c(new dg_gpu_ctx());
   c->device = o.device;
+  c->num_sms = prop.multiProcessorCount;
   c->precision = o.precision;
   c->is_double = o.precision == DG_FP64_REF || o.precision == DG_FP64;
   c->kahan = o.precision == DG_FP32_KAHAN;
@@ -727,7 +947,11 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
     choose_kind(meshes[k].n_shots, meshes[k].K, !c->is_double, o.variant, p.kind, p.S_pad);
     if (o.variant == 2 && p.kind == 0)
       return fail(DG_ERR_UNSUPPORTED, "no packed FP32 kernel for this mesh (FP32 only; at most 128 shots)");
-    int rc = prepare(meshes[k], o.precision, o.reorder, p);
+    // the wavefront step: one FP32 mesh on the two-shot kernels; automatic = on
+    c->wave = !c->multi && p.kind == 2 && wave_supported(p.S_pad) && o.wavefront != -1;
+    if (o.wavefront == 1 && !c->wave)
+      return fail(DG_ERR_UNSUPPORTED, "the wavefront step needs one FP32 mesh with 2, 4, 8, ..., 128 shots");
+    int rc = prepare(meshes[k], o.precision, c->wave ? 2 : o.reorder, p);
     if (rc) return rc;
     MeshHostInfo& h = c->mi[k];
     h.K = p.K;
@@ -736,6 +960,10 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
     h.S_pad = p.S_pad;
     h.kind = p.kind;
     if (!c->multi) c->x2 = p.kind == 1 ? 1 : (p.kind == 2 ? p.S_pad : 0);
+    if (c->wave) {
+      c->face_h = p.face;
+      c->rec_elem_h = p.rec_elem;
+    }
     h.n_rec = p.n_rec;
     h.steps = meshes[k].n_steps;
     h.dt = meshes[k].dt;
@@ -755,11 +983,14 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
     // geo (2 x 4 values), 1/rho (1 value), lambda/mu/lambda+2mu (4 values) and face codes (2 x 16 B)
     double per = 90.0 * h.S * w + (c->kahan ? 60.0 * h.S * 4 : 0.0) + 13.0 * w + 32.0;
     if (o.precision == DG_FP64_REF) per = 90.0 * h.S * 8 + 2.0 * 72 * 8 + 30 * 8 + 10 * 8 + 32.0;
+    // the wavefront step reads and writes each of the 30 values once (the rest is L2 traffic)
+    const double per_wave = 60.0 * h.S * w + (c->kahan ? 60.0 * h.S * 4 : 0.0) + 13.0 * w + 32.0;
     bytes += per * (double)h.K;
+    c->bytes_wave += per_wave * (double)h.K;
     dof += 30.0 * (double)h.K * h.S;
     stage = std::max(stage, (size_t)std::max<long>(h.K * 6, h.steps * std::max(1, h.n_rec)));
   }
-  c->stats.bytes_per_step = bytes;
+  c->bytes_two_pass = bytes;
   c->stats.dof_per_step = dof;
   if (c->is_double) fill_ops(c->ops_d, meshes[0]); else fill_ops(c->ops_f, meshes[0]);
   for (int q = 0; q < 36; q++) {
@@ -775,7 +1006,9 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   c->stage_elems = stage;
   CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), c->stream));
 
-  int block = o.block_threads ? o.block_threads : 256;
+  // automatic block size: 64 threads for the packed two-shot kernels (one or two elements per
+  // warp, so small blocks spread a chunk's neighbours over more SMs), 256 otherwise
+  int block = o.block_threads ? o.block_threads : (c->x2 >= 2 ? 64 : 256);
   if ((rc = set_block(c.get(), block))) return rc;
   if (o.autotune && !o.block_threads)
     if ((rc = autotune(c.get(), o.tune_cache))) return rc;
@@ -812,7 +1045,7 @@ static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
         c->stats.ms_velocity += a;
         c->stats.ms_stress += b;
       }
-      c->stats.launches += 2 * chunk;
+      c->stats.launches += (c->wave ? 1 : 2) * chunk;
     } else {
       long k = 0;
       if (c->graph && c->graph_steps > 0)
@@ -821,7 +1054,7 @@ static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
         int rc = launch_step(c);
         if (rc) return rc;
       }
-      c->stats.launches += 2 * chunk;
+      c->stats.launches += (c->wave ? 1 : 2) * chunk;
     }
     done += chunk;
     c->t += chunk;
@@ -841,7 +1074,7 @@ static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
   }
   CK(cudaStreamSynchronize(c->stream));
   c->stats.steps_done = c->t;
-  return DG_OK;
+  return check_wave(c);
 }
 
 int dg_gpu_step(dg_gpu_ctx* c, long n) { return do_steps(c, n, false); }
@@ -902,9 +1135,9 @@ int dg_gpu_step_profiled(dg_gpu_ctx* c, long n, int flush_l2, float* ms_vel, flo
   c->t += n;
   c->stats.ms_velocity = sv;
   c->stats.ms_stress = ss;
-  c->stats.launches = 2 * n;
+  c->stats.launches = (c->wave ? 1 : 2) * n;
   c->stats.steps_done = c->t;
-  return DG_OK;
+  return check_wave(c);
 }
 
 int dg_gpu_fetch_traces(dg_gpu_ctx* c, int mesh, long t0, long n, double* dst_x, double* dst_z) {
@@ -1028,7 +1261,8 @@ int dg_gpu_stats_get(dg_gpu_ctx* c, dg_gpu_stats* out) {
   c->stats.block_threads = c->block;
   c->stats.graph_steps = c->graph_steps;
   c->stats.kernel_family =
-      c->precision == DG_FP64_REF ? 0 : (c->mx ? 4 : (c->x2 == 1 ? 3 : (c->x2 ? 2 : 1)));
+      c->precision == DG_FP64_REF ? 0 : (c->wave ? 5 : (c->mx ? 4 : (c->x2 == 1 ? 3 : (c->x2 ? 2 : 1))));
+  c->stats.bytes_per_step = c->wave ? c->bytes_wave : c->bytes_two_pass;
   *out = c->stats;
   return DG_OK;
 }

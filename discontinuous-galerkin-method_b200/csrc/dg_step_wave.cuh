@@ -1,0 +1,144 @@
+// dg_step_wave.cuh — the whole time step (sponge, source, velocity, stress, record) in one launch,
+// as a wavefront that keeps the state of the elements in flight in L2.
+//
+// Elements are numbered in a bandwidth-reducing (reverse Cuthill-McKee) order.  The unit of work
+// is one warp's share of the element range (32 threads, two shots each).  A block takes a ticket
+// tau (an atomic counter, so tickets follow the order in which blocks start) and each of its warps
+// does two pieces of work, with no barrier between them:
+//   * the velocity update of its unit in block tau, the receivers of that unit, then publishes
+//     flag[unit] = step id;
+//   * the stress update of its unit in block tau - L, after waiting until every unit holding one of
+//     that unit's elements or their neighbours has published the flag.
+// The stress update of a unit overwrites stresses that only those velocity updates read, so the
+// in-place update is safe.  L is at least the unit bandwidth in blocks, so a warp only ever waits
+// on units of lower or equal tickets, whose warps are running or done and never wait before
+// publishing — no cycle, no deadlock, co-residency not required.  Each wait is bounded: past the
+// limit (or once any warp gave up) the warp sets the error word and carries on, and the host
+// reports the error.  With the lag window in L2, each state value crosses HBM about once per step:
+// 30 reads and 30 writes per element and shot instead of the 90 of two separate passes.
+#pragma once
+#include "dg_common.cuh"
+#include "dg_step_x2.cuh"
+
+#ifndef DG_WAVE_MINB
+#define DG_WAVE_MINB 2  // resident 256-thread blocks per SM the register budget is cut for
+#endif
+
+namespace dg {
+
+struct Wave {
+  int NU;                 // warp units: ceil(K * S/2 / 32)
+  int NB;                 // blocks of units: ceil(NU / warps per block)
+  int L;                  // lag between a unit's velocity and its stress work, in blocks
+  int W;                  // wait-list width (<= 32)
+  const int* wait;        // [NU][W] units holding the unit's elements or their neighbours, -1 padded
+  unsigned int* vflag;    // [NU] step id (t + 1) once the unit's new velocities are stored
+  const int* rec_start;   // [NU + 1] receivers whose element the unit covers:
+  const int* rec_list;    //   rec_list[rec_start[u] .. rec_start[u+1])
+  unsigned long long* tickets;  // blocks started since step 0: launch t hands out t*G .. t*G + G - 1
+  int* error;             // bit 0: a wait reached its limit
+  unsigned int spin_limit;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_volatile_i32(const int* p) { return *(volatile const int*)p; }
+
+// Receivers of unit u right after its velocity update (Record, OpenMP_Function.c:61-72): each
+// thread stores the two shots it has just updated, so it reads back only its own stores.
+template <int S>
+__device__ __forceinline__ void record_unit(const MeshDev<float>& m, const Wave& w, int u, int r0, int r1,
+                                            long long t) {
+  constexpr int H = S / 2;
+  const int g = u * 32 + (int)(threadIdx.x & 31);
+  const int e = g / H, lane = g - e * H;
+  float* tx = m.trace + (t * 2) * (long long)m.n_rec * S;
+  float* tz = tx + (long long)m.n_rec * S;
+  for (int q = r0; q < r1; q++) {
+    const int rr = __ldg(w.rec_list + q);
+    if (__ldg(m.rec_elem + rr) != e) continue;
+    const int node = __ldg(m.rec_node + rr);
+    const float2* Ue = reinterpret_cast<const float2*>(m.U) + (long long)e * 30 * H + lane;
+    reinterpret_cast<float2*>(tx + (long long)rr * S)[lane] = Ue[node * H];
+    reinterpret_cast<float2*>(tz + (long long)rr * S)[lane] = Ue[(6 + node) * H];
+  }
+}
+
+// Each lane waits on one unit of the wait list (k < 0: none) to publish step id.
+__device__ __forceinline__ void wait_units(const Wave& w, int k, unsigned id) {
+  if (k >= 0) {
+    unsigned spins = 0;
+    while (ld_acquire_u32(w.vflag + k) != id) {
+      if (++spins > w.spin_limit || (ld_volatile_i32(w.error) & 1)) {
+        atomicOr(w.error, 1);
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  __syncwarp();
+}
+
+// Sets the ticket counter to the step the counters hold, for a launch grid of G blocks.
+__global__ void k_wave_sync(const Counters* __restrict__ ctr, unsigned long long* tickets, unsigned G) {
+  *tickets = (unsigned long long)ctr->v * G;
+}
+
+template <int S, bool KAHAN>
+__global__ void __launch_bounds__(256, DG_WAVE_MINB) k_step_wave(const __grid_constant__ Ops2 ops,
+                                                                 const __grid_constant__ MeshDev<float> m,
+                                                                 const __grid_constant__ Wave w,
+                                                                 Counters* __restrict__ ctr) {
+  __shared__ unsigned long long s_tk;
+  if (threadIdx.x == 0) s_tk = atomicAdd(w.tickets, 1ull);
+  __syncthreads();
+  // the ticket gives both the step and the block's place in it, so no block reads the counters
+  // and none has to rewind anything at the end of the launch
+  const long long t = (long long)(s_tk / gridDim.x);
+  const int tau = (int)(s_tk - (unsigned long long)t * gridDim.x);
+  if (tau == 0 && threadIdx.x == 0) {
+    ctr->v = t + 1;
+    ctr->s = t + 1;
+  }
+  if (t >= m.steps) return;
+  const unsigned id = (unsigned)(t + 1);
+  const int wpb = (int)(blockDim.x >> 5), warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+  const int uv = tau * wpb + warp, j = tau - w.L, ut = j * wpb + warp;
+  const bool do_v = tau < w.NB && uv < w.NU;
+  const bool do_t = j >= 0 && j < w.NB && ut < w.NU;
+  // the stress unit's wait list and the velocity unit's receiver range are fetched before the
+  // velocity work, so their latency hides behind it
+  const int k = (do_t && lane < w.W) ? __ldg(w.wait + (long long)ut * w.W + lane) : -1;
+  int r0 = 0, r1 = 0;
+  if (do_v) {
+    r0 = __ldg(w.rec_start + uv);
+    r1 = __ldg(w.rec_start + uv + 1);
+  }
+  if (do_v) {
+    velocity_x2_body<S, KAHAN>(ops, m, tau, t);
+    __syncwarp();
+    if (r0 != r1) record_unit<S>(m, w, uv, r0, r1, t);
+    __syncwarp();
+  }
+  // the stress element's constants are requested before the release and the wait, which they
+  // overlap (a thread past the last element reads the last element's and discards them)
+  constexpr int H = S / 2;
+  const int g = j * (int)blockDim.x + (int)threadIdx.x;
+  const int e = min(g / H, m.K - 1), q = g - (g / H) * H;
+  StressConst sc;
+  if (do_t) sc = stress_const(m, e);
+  // the warp barrier above orders every lane's stores before lane 0's release
+  if (do_v && lane == 0) st_release_u32(w.vflag + uv, id);
+  if (do_t) {
+    wait_units(w, k, id);
+    if (g < m.K * H) stress_x2_core<S, KAHAN, true>(ops, m, e, q, sc);
+  }
+}
+
+}  // namespace dg

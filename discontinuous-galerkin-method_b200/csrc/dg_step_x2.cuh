@@ -209,21 +209,37 @@ __global__ void __launch_bounds__(256, 2) k_velocity_x2(const __grid_constant__ 
   velocity_x2_body<S, KAHAN>(ops, m, blockIdx.x, t);
 }
 
-template <int S, bool KAHAN>
-__device__ __forceinline__ void stress_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
+// Load of a velocity value: plain, or through L2 (FRESH) when other blocks of the same launch
+// wrote it (the wavefront step), so no stale L1 line can be returned.
+template <bool FRESH>
+__device__ __forceinline__ float2 ld_v(const float2* p) {
+  if (FRESH) return __ldcg(p);
+  return *p;
+}
+
+// The per-element constants of the stress update: face codes, geometric factors, materials.
+struct StressConst {
+  int4 fc;
+  float4 gm, mt;
+};
+__device__ __forceinline__ StressConst stress_const(const MeshDev<float>& m, int e) {
+  return {__ldg(m.face + e), __ldg(m.geo + e), __ldg(m.mat + e)};
+}
+
+// Stress update of lane q (shots 2q, 2q+1) of element e with its constants already loaded.
+template <int S, bool KAHAN, bool FRESH>
+__device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<float>& m, int e, int q,
+                                               const StressConst& k) {
   constexpr int H = S / 2;
   constexpr int ES = 30 * H;
-  const int g = lb * blockDim.x + threadIdx.x;
-  if (g >= m.K * H) return;
-  const int e = g / H, q = g - e * H;
   float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * ES + q;
 
   float2 vx[NP], vz[NP];
 #pragma unroll
-  for (int i = 0; i < NP; i++) { vx[i] = Ue[(0 + i) * H]; vz[i] = Ue[(6 + i) * H]; }
-  const int4 fc = __ldg(m.face + e);
-  const float4 gm = __ldg(m.geo + e);
-  const float4 mt = __ldg(m.mat + e);
+  for (int i = 0; i < NP; i++) { vx[i] = ld_v<FRESH>(Ue + (0 + i) * H); vz[i] = ld_v<FRESH>(Ue + (6 + i) * H); }
+  const int4 fc = k.fc;
+  const float4 gm = k.gm;
+  const float4 mt = k.mt;
   const float2 rx = f2(gm.x), sx = f2(gm.y), rz = f2(gm.z), sz = f2(gm.w);
 
   // volume: X = dxVx, Z = dzVz, W = dxVz + dzVx
@@ -262,8 +278,8 @@ __device__ __forceinline__ void stress_x2_body(const Ops2& ops, const MeshDev<fl
 #pragma unroll
       for (int k = 0; k < NF; k++) {
         const int node = face_node(nf, flip ? 2 - k : k);
-        px[k] = Un[(0 + node) * H];
-        pz[k] = Un[(6 + node) * H];
+        px[k] = ld_v<FRESH>(Un + (0 + node) * H);
+        pz[k] = ld_v<FRESH>(Un + (6 + node) * H);
       }
     }
     float2 fa[NF], fb[NF], fw[NF];
@@ -333,6 +349,15 @@ __device__ __forceinline__ void stress_x2_body(const Ops2& ops, const MeshDev<fl
       Ce[(12 + i) * H] = cxx[i]; Ce[(18 + i) * H] = czz[i]; Ce[(24 + i) * H] = cxz[i];
     }
   }
+}
+
+template <int S, bool KAHAN, bool FRESH = false>
+__device__ __forceinline__ void stress_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
+  constexpr int H = S / 2;
+  const int g = lb * blockDim.x + threadIdx.x;
+  if (g >= m.K * H) return;
+  const int e = g / H, q = g - e * H;
+  stress_x2_core<S, KAHAN, FRESH>(ops, m, e, q, stress_const(m, e));
 }
 
 template <int S, bool KAHAN>

@@ -20,7 +20,7 @@ FIELDS = {"Vx": VX, "Vz": VZ, "Txx": TXX, "Tzz": TZZ, "Txz": TXZ}
 
 ERRORS = {0: "DG_OK", -1: "DG_ERR_ARG", -2: "DG_ERR_CUDA", -3: "DG_ERR_NOMEM", -4: "DG_ERR_MESH",
           -5: "DG_ERR_NONFINITE", -6: "DG_ERR_STATE", -7: "DG_ERR_UNSUPPORTED", -8: "DG_ERR_NODEVICE",
-          -9: "DG_ERR_ORIENTATION"}
+          -9: "DG_ERR_ORIENTATION", -10: "DG_ERR_TIMEOUT"}
 
 # exported symbols of include/dg_gpu.h (checked by the CPU tests)
 def _ptr(a):
@@ -69,7 +69,7 @@ class _Mesh(C.Structure):
 class _Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("reorder", C.c_int), ("block_threads", C.c_int),
                 ("graph_steps", C.c_int), ("autotune", C.c_int), ("watchdog_every", C.c_int),
-                ("tune_cache", C.c_char_p), ("variant", C.c_int)]
+                ("tune_cache", C.c_char_p), ("variant", C.c_int), ("wavefront", C.c_int)]
 
 
 class _Stats(C.Structure):
@@ -81,10 +81,11 @@ KERNEL_FAMILIES = {0: "reference operators (k_velocity_ref/k_stress_ref)",
                    1: "one (element, shot) per thread (k_velocity/k_stress)",
                    2: "two shots per thread, packed FP32x2 (k_velocity_x2/k_stress_x2)",
                    3: "two elements per thread, packed FP32x2 (k_velocity_x2e/k_stress_x2e)",
-                   4: "batch of meshes, each block on its mesh's packed body (k_velocity_mx/k_stress_mx)"}
+                   4: "batch of meshes, each block on its mesh's packed body (k_velocity_mx/k_stress_mx)",
+                   5: "wavefront step: one launch per step, two shots per thread, L2-resident lag (k_step_wave)"}
 KERNEL_NAMES = {0: ("k_velocity_ref", "k_stress_ref"), 1: ("k_velocity", "k_stress"),
                 2: ("k_velocity_x2", "k_stress_x2"), 3: ("k_velocity_x2e", "k_stress_x2e"),
-                4: ("k_velocity_mx", "k_stress_mx")}
+                4: ("k_velocity_mx", "k_stress_mx"), 5: ("k_step_wave", None)}
 
 
 _LIB = None
@@ -158,7 +159,7 @@ class Engine:
     """One device context over one or more meshes (all meshes step together)."""
 
     def __init__(self, meshes, precision="fp64", *, device=0, reorder=True, block_threads=0, graph_steps=0,
-                 autotune=False, watchdog_every=0, tune_cache=None, variant=0):
+                 autotune=False, watchdog_every=0, tune_cache=None, variant=0, wavefront=0):
         if isinstance(meshes, dict):
             meshes = [meshes]
         prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
@@ -197,6 +198,7 @@ class Engine:
         opts.watchdog_every = watchdog_every
         opts.tune_cache = tune_cache.encode() if tune_cache else None
         opts.variant = int(variant)
+        opts.wavefront = int(wavefront)
         self._ctx = C.c_void_p()
         _check(lib().dg_gpu_init(C.byref(self._ctx), arr, len(meshes), C.byref(opts)), "dg_gpu_init")
         self._keep = []

@@ -34,6 +34,7 @@ extern "C" {
 #define DG_ERR_UNSUPPORTED -7  /* Np != 6, Nfp != 3, more meshes than supported */
 #define DG_ERR_NODEVICE -8     /* no CUDA device, or not an sm_100 device */
 #define DG_ERR_ORIENTATION -9  /* a triangle with non-positive Jacobian (compact paths need CCW) */
+#define DG_ERR_TIMEOUT -10     /* a wait between blocks of a wavefront step reached its limit */
 
 /* arithmetic of the time loop */
 #define DG_FP64_REF 0    /* the reference's per-element Dx/Dz/Q/A/B arrays, its operation order,
@@ -95,8 +96,10 @@ typedef struct {
 	int autotune;        /* 1: time candidate block sizes at init */
 	int watchdog_every;  /* check the velocity fields for NaN/Inf every k steps (0: off) */
 	const char *tune_cache; /* file that keeps autotune results between runs (NULL: none) */
-	int variant;         /* FP32 kernels: 0 automatic, 1 one shot per thread (plane-major layout),
-	                        2 two shots per thread with packed FP32x2 (needs n_shots in {2,4,...,128}) */
+	int variant;         /* FP32 kernels: 0 automatic, 1 one (element, shot) per thread,
+	                        2 packed FP32x2 kernels (two elements or two shots per thread) */
+	int wavefront;       /* one launch per step that keeps the state in flight in L2 (single FP32 mesh
+	                        with 2 or more shots): 0 automatic, 1 on, -1 off */
 } dg_gpu_opts;
 
 typedef struct {
@@ -110,7 +113,8 @@ typedef struct {
 	double dof_per_step;   /* 30 * sum over meshes of K * n_shots */
 	int kernel_family;     /* 0 reference operators, 1 one (element, shot) per thread,
 	                          2 two shots per thread (packed FP32x2), 3 two elements per thread (packed),
-	                          4 FP32 batch of meshes, each block running its mesh's packed body */
+	                          4 FP32 batch of meshes, each block running its mesh's packed body,
+	                          5 wavefront step (one launch per step, two shots per thread) */
 } dg_gpu_stats;
 
 void dg_gpu_default_opts(dg_gpu_opts *opts);

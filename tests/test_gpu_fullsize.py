@@ -121,21 +121,18 @@ def test_multishot_batch_properties():
         e1.step(w.steps)
         assert np.array_equal(_traces(e1), batch_shot)
         assert np.array_equal(e1.fetch("Txz"), batch_field)
-    # doubling the source doubles every value: exactly in FP64; in FP32 up to the rounding of
-    # underflowed values ahead of the wave front (their relative error is carried along as the
-    # front grows), measured here in relative L2
+    # doubling the source doubles every value up to the rounding of values that underflow ahead
+    # of the wave front (their relative error is carried along as the front grows; on this mesh
+    # the precursor reaches the FP64 subnormal range too), measured in relative L2
     m2 = dict(m)
     m2["wavelet"] = 2.0 * m["wavelet"]
-    for p, tol in (("fp64", 0.0), ("fp32", 1e-6)):
+    for p, tol in (("fp64", 1e-12), ("fp32", 1e-6)):
         with eng.Engine(m, p) as a, eng.Engine(m2, p) as b:
             a.step(300)
             b.step(300)
             for shot in (0, 40):
                 ta, tb = 2.0 * _traces(a, 0, shot), _traces(b, 0, shot)
-                if tol == 0.0:
-                    assert np.array_equal(ta, tb)
-                else:
-                    assert rel_l2(ta, tb) <= tol, rel_l2(ta, tb)
+                assert rel_l2(ta, tb) <= tol, (p, rel_l2(ta, tb))
 
 
 def test_uneven_batch_each_mesh_against_fp64_and_own_step_count():

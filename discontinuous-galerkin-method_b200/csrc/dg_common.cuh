@@ -31,6 +31,34 @@ __host__ __device__ __forceinline__ int face_node(int j, int k) {
   return (int)((FACE_NODES >> (4 * (3 * j + k))) & 15ULL);
 }
 
+// The P2 operators on the reference triangle for the node order of the reference's operator
+// files (FeketeNew: (1,-1), (0,0), (-1,1), (0,-1), (-1,0), (-1,-1)).  Every entry is a multiple
+// of 1/8: the files hold them to 8 digits, these are the exact values.  Dr = Vr inv(V) and
+// Ds = Vs inv(V) each have 22 nonzeros of 36; p2_lift((j*6 + i)*3 + k) is S_j (face-j lift).  The packed
+// FP32 bodies take their operators from here as compile-time constants (zeros skipped, +-1 as an
+// add or a subtract); the host checks the operators it is given against them first.
+__host__ __device__ constexpr float p2_dr(int q) {
+  constexpr float v[36] = {1.5f,  0.f, 0.f, -2.f, 0.f,  0.5f,  0.5f, 1.f, 0.f, -1.f, -1.f, 0.5f,
+                             -0.5f, 2.f, 0.f, 0.f,  -2.f, 0.5f,  0.5f, 0.f, 0.f, 0.f,  0.f,  -0.5f,
+                             -0.5f, 1.f, 0.f, 1.f,  -1.f, -0.5f, -0.5f, 0.f, 0.f, 2.f, 0.f,  -1.5f};
+  return v[q];
+}
+__host__ __device__ constexpr float p2_ds(int q) {
+  constexpr float v[36] = {0.f, 2.f, -0.5f, -2.f, 0.f,  0.5f,  0.f, 1.f, 0.5f,  -1.f, -1.f, 0.5f,
+                             0.f, 0.f, 1.5f,  0.f,  -2.f, 0.5f,  0.f, 1.f, -0.5f, -1.f, 1.f,  -0.5f,
+                             0.f, 0.f, 0.5f,  0.f,  0.f,  -0.5f, 0.f, 0.f, -0.5f, 0.f,  2.f,  -1.5f};
+  return v[q];
+}
+__host__ __device__ constexpr float p2_lift(int q) {
+  constexpr float v[54] = {-0.5f,   2.f,   4.5f,   0.625f,  -1.5f, -0.625f, 1.f,    4.f,  1.f,
+                               0.5f,    5.f,   0.5f,   -0.625f, -1.5f, 0.625f,  4.5f,   2.f,  -0.5f,
+                               4.5f,    2.f,   -0.5f,  0.5f,    5.f,   0.5f,    -0.5f,  2.f,  4.5f,
+                               -0.625f, -1.5f, 0.625f, 0.625f,  -1.5f, -0.625f, 1.f,    4.f,  1.f,
+                               1.f,     4.f,   1.f,    0.625f,  -1.5f, -0.625f, -0.5f,  2.f,  4.5f,
+                               -0.625f, -1.5f, 0.625f, 0.5f,    5.f,   0.5f,    4.5f,   2.f,  -0.5f};
+  return v[q];
+}
+
 template <class R> struct R4T;
 template <> struct R4T<float> { using type = float4; };
 template <> struct R4T<double> { using type = double4; };

@@ -485,6 +485,27 @@ int upload_mesh(dg_gpu_ctx* c, const dg_gpu_mesh& m, Prepared& p, MeshDev<R>& d)
   return DG_OK;
 }
 
+// True when the mesh's operators equal the compile-time P2 tables of the packed FP32 kernels:
+// Dr = Vr inv(V), Ds = Vs inv(V) and the face lifts S_j, each entry to 1e-6 of the largest.
+bool p2_operators_match(const dg_gpu_mesh& m) {
+  double big = 0, err = 0;
+  for (int i = 0; i < 6; i++)
+    for (int q = 0; q < 6; q++) {
+      double a = 0, b = 0;
+      for (int k = 0; k < 6; k++) {
+        a += m.Vr[i * 6 + k] * m.inverV[k * 6 + q];
+        b += m.Vs[i * 6 + k] * m.inverV[k * 6 + q];
+      }
+      big = std::max(big, std::max(std::fabs(a), std::fabs(b)));
+      err = std::max(err, std::max(std::fabs(a - p2_dr(i * 6 + q)), std::fabs(b - p2_ds(i * 6 + q))));
+    }
+  for (int q = 0; q < 54; q++) {
+    big = std::max(big, std::fabs(m.S[q]));
+    err = std::max(err, std::fabs(m.S[q] - p2_lift(q)));
+  }
+  return err <= 1e-6 * big;
+}
+
 template <class R> void fill_ops(Ops<R>& o, const dg_gpu_mesh& m) {
   // Dr = Vr inv(V), Ds = Vs inv(V) from the parsed operator files
   for (int i = 0; i < 6; i++)
@@ -623,6 +644,7 @@ int build_wave(dg_gpu_ctx* c) {
   w.spin_limit = 1u << 20;  // a million polls of an L2 line: well under a second
   c->blocks_v = NB + w.L;
   c->blocks_t = 0;
+  w.inv_G = ~0ULL / (unsigned long long)c->blocks_v;
   k_wave_sync<<<1, 1, 0, c->stream>>>(c->d_ctr, d_tk, (unsigned)c->blocks_v);
   CK(cudaGetLastError());
   return DG_OK;
@@ -942,9 +964,16 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   double bytes = 0, dof = 0;
   size_t stage = 1;
   const size_t w = c->is_double ? 8 : 4;
+  // the packed FP32 kernels carry the P2 operators as compile-time constants: other operators
+  // run on the one-(element, shot)-per-thread kernels
+  bool p2_ok = true;
+  for (int k = 0; k < n_meshes; k++) p2_ok = p2_ok && p2_operators_match(meshes[k]);
+  const int variant = (!c->is_double && !p2_ok && o.variant != 2) ? 1 : o.variant;
+  if (o.variant == 2 && !c->is_double && !p2_ok)
+    return fail(DG_ERR_UNSUPPORTED, "the packed FP32 kernels need the P2 operators of the reference triangle");
   for (int k = 0; k < n_meshes; k++) {
     Prepared p;
-    choose_kind(meshes[k].n_shots, meshes[k].K, !c->is_double, o.variant, p.kind, p.S_pad);
+    choose_kind(meshes[k].n_shots, meshes[k].K, !c->is_double, variant, p.kind, p.S_pad);
     if (o.variant == 2 && p.kind == 0)
       return fail(DG_ERR_UNSUPPORTED, "no packed FP32 kernel for this mesh (FP32 only; at most 128 shots)");
     // the wavefront step: one FP32 mesh on the two-shot kernels; automatic = on

@@ -21,7 +21,10 @@
 #include "dg_step_x2.cuh"
 
 #ifndef DG_WAVE_MINB
-#define DG_WAVE_MINB 2  // resident 256-thread blocks per SM the register budget is cut for
+#define DG_WAVE_MINB 2  // resident blocks of DG_WAVE_MAXT threads per SM the register budget is cut for
+#endif
+#ifndef DG_WAVE_MAXT
+#define DG_WAVE_MAXT 256
 #endif
 
 namespace dg {
@@ -38,6 +41,7 @@ struct Wave {
   unsigned long long* tickets;  // blocks started since step 0: launch t hands out t*G .. t*G + G - 1
   int* error;             // bit 0: a wait reached its limit
   unsigned int spin_limit;
+  unsigned long long inv_G;  // floor((2^64 - 1) / G), G = blocks of the launch
 };
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -91,17 +95,25 @@ __global__ void k_wave_sync(const Counters* __restrict__ ctr, unsigned long long
 }
 
 template <int S, bool KAHAN>
-__global__ void __launch_bounds__(256, DG_WAVE_MINB) k_step_wave(const __grid_constant__ Ops2 ops,
+__global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave(const __grid_constant__ Ops2 ops,
                                                                  const __grid_constant__ MeshDev<float> m,
                                                                  const __grid_constant__ Wave w,
                                                                  Counters* __restrict__ ctr) {
-  __shared__ unsigned long long s_tk;
-  if (threadIdx.x == 0) s_tk = atomicAdd(w.tickets, 1ull);
+  __shared__ long long s_t;
+  __shared__ int s_tau;
+  if (threadIdx.x == 0) {
+    // the ticket gives both the step (ticket / G) and the block's place in it, so no block reads
+    // the counters and none has to rewind anything at the end of the launch; the quotient comes
+    // from the reciprocal, one short of the true one at most
+    const unsigned long long tk = atomicAdd(w.tickets, 1ull), G = gridDim.x;
+    unsigned long long q = __umul64hi(tk, w.inv_G);
+    if (tk - q * G >= G) q++;
+    s_t = (long long)q;
+    s_tau = (int)(tk - q * G);
+  }
   __syncthreads();
-  // the ticket gives both the step and the block's place in it, so no block reads the counters
-  // and none has to rewind anything at the end of the launch
-  const long long t = (long long)(s_tk / gridDim.x);
-  const int tau = (int)(s_tk - (unsigned long long)t * gridDim.x);
+  const long long t = s_t;
+  const int tau = s_tau;
   if (tau == 0 && threadIdx.x == 0) {
     ctr->v = t + 1;
     ctr->s = t + 1;

@@ -10,7 +10,8 @@ namespace dg {
 // element-major with shots innermost, U[e][plane][S], so thread q of an element owns shots 2q and
 // 2q+1 as one float2 and all 30 planes of its element sit at compile-time offsets (multiples of
 // S/2 float2) from one base address; a neighbour's planes likewise from nb * 30 * S/2.  The
-// operator constants come pre-duplicated as float2 pairs so they feed the packed FMAs directly.
+// operators are the compile-time P2 tables (p2_dr, p2_ds, p2_lift), so no operator value is
+// loaded at run time.
 struct Ops2 {
   float2 Dr[NP * NP];
   float2 Ds[NP * NP];
@@ -23,6 +24,15 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 // a - b, exactly rounded (b * -1 is exact)
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+
+// h + c x for an operator entry c known at compile time: nothing for 0, an add or a subtract for
+// +-1 (the same rounding as the FMA), a packed FMA otherwise
+__device__ __forceinline__ float2 axpy_c(float c, float2 x, float2 h) {
+  if (c == 0.f) return h;
+  if (c == 1.f) return add2(h, x);
+  if (c == -1.f) return sub2(h, x);
+  return fma2(f2(c), x, h);
+}
 
 // Kahan-compensated u += d with compensation c (both lanes)
 __device__ __forceinline__ void kahan2(float2& u, float2& c, float2 d) {
@@ -112,41 +122,31 @@ __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<
     for (int i = 0; i < NP; i++)
 #pragma unroll
       for (int k = 0; k < NF; k++) {
-        hx[i] = fma2(ops.L[(j * NP + i) * NF + k], fx[k], hx[i]);
-        hz[i] = fma2(ops.L[(j * NP + i) * NF + k], fz[k], hz[i]);
+        hx[i] = axpy_c(p2_lift((j * NP + i) * NF + k), fx[k], hx[i]);
+        hz[i] = axpy_c(p2_lift((j * NP + i) * NF + k), fz[k], hz[i]);
       }
   }
 
-  // volume terms: Dr (rx Txx + rz Txz) + Ds (sx Txx + sz Txz) and the same for (Txz, Tzz)
+  // volume terms: Dr (rx Txx + rz Txz) + Ds (sx Txx + sz Txz) and the same for (Txz, Tzz); each
+  // nonzero operator entry is read once and serves both components
   const float2 rx = f2(gm.x), sx = f2(gm.y), rz = f2(gm.z), sz = f2(gm.w);
   {
-    float2 a[NP], b[NP];
+    float2 a[NP], b[NP], c[NP], d[NP];
 #pragma unroll
     for (int n = 0; n < NP; n++) {
       a[n] = fma2(rx, txx[n], mul2(rz, txz[n]));
       b[n] = fma2(sx, txx[n], mul2(sz, txz[n]));
+      c[n] = fma2(rx, txz[n], mul2(rz, tzz[n]));
+      d[n] = fma2(sx, txz[n], mul2(sz, tzz[n]));
     }
 #pragma unroll
     for (int i = 0; i < NP; i++)
 #pragma unroll
       for (int n = 0; n < NP; n++) {
-        hx[i] = fma2(ops.Dr[i * NP + n], a[n], hx[i]);
-        hx[i] = fma2(ops.Ds[i * NP + n], b[n], hx[i]);
-      }
-  }
-  {
-    float2 a[NP], b[NP];
-#pragma unroll
-    for (int n = 0; n < NP; n++) {
-      a[n] = fma2(rx, txz[n], mul2(rz, tzz[n]));
-      b[n] = fma2(sx, txz[n], mul2(sz, tzz[n]));
-    }
-#pragma unroll
-    for (int i = 0; i < NP; i++)
-#pragma unroll
-      for (int n = 0; n < NP; n++) {
-        hz[i] = fma2(ops.Dr[i * NP + n], a[n], hz[i]);
-        hz[i] = fma2(ops.Ds[i * NP + n], b[n], hz[i]);
+        hx[i] = axpy_c(p2_dr(i * NP + n), a[n], hx[i]);
+        hz[i] = axpy_c(p2_dr(i * NP + n), c[n], hz[i]);
+        hx[i] = axpy_c(p2_ds(i * NP + n), b[n], hx[i]);
+        hz[i] = axpy_c(p2_ds(i * NP + n), d[n], hz[i]);
       }
   }
 
@@ -249,10 +249,10 @@ __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<fl
     float2 drx = f2(0.f), dsx = f2(0.f), drz = f2(0.f), dsz = f2(0.f);
 #pragma unroll
     for (int n = 0; n < NP; n++) {
-      drx = fma2(ops.Dr[i * NP + n], vx[n], drx);
-      dsx = fma2(ops.Ds[i * NP + n], vx[n], dsx);
-      drz = fma2(ops.Dr[i * NP + n], vz[n], drz);
-      dsz = fma2(ops.Ds[i * NP + n], vz[n], dsz);
+      drx = axpy_c(p2_dr(i * NP + n), vx[n], drx);
+      drz = axpy_c(p2_dr(i * NP + n), vz[n], drz);
+      dsx = axpy_c(p2_ds(i * NP + n), vx[n], dsx);
+      dsz = axpy_c(p2_ds(i * NP + n), vz[n], dsz);
     }
     X[i] = fma2(rx, drx, mul2(sx, dsx));
     Z[i] = fma2(rz, drz, mul2(sz, dsz));
@@ -296,10 +296,10 @@ __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<fl
     for (int i = 0; i < NP; i++)
 #pragma unroll
       for (int k = 0; k < NF; k++) {
-        const float2 l = ops.L[(j * NP + i) * NF + k];
-        X[i] = fma2(l, fa[k], X[i]);
-        Z[i] = fma2(l, fb[k], Z[i]);
-        W[i] = fma2(l, fw[k], W[i]);
+        const float l = p2_lift((j * NP + i) * NF + k);
+        X[i] = axpy_c(l, fa[k], X[i]);
+        Z[i] = axpy_c(l, fb[k], Z[i]);
+        W[i] = axpy_c(l, fw[k], W[i]);
       }
   }
 
@@ -469,8 +469,8 @@ __device__ __forceinline__ void velocity_x2e_body(const Ops2& ops, const MeshDev
     for (int i = 0; i < NP; i++)
 #pragma unroll
       for (int k = 0; k < NF; k++) {
-        hx[i] = fma2(ops.L[(j * NP + i) * NF + k], fx[k], hx[i]);
-        hz[i] = fma2(ops.L[(j * NP + i) * NF + k], fz[k], hz[i]);
+        hx[i] = axpy_c(p2_lift((j * NP + i) * NF + k), fx[k], hx[i]);
+        hz[i] = axpy_c(p2_lift((j * NP + i) * NF + k), fz[k], hz[i]);
       }
   }
   {
@@ -486,10 +486,10 @@ __device__ __forceinline__ void velocity_x2e_body(const Ops2& ops, const MeshDev
     for (int i = 0; i < NP; i++)
 #pragma unroll
       for (int n = 0; n < NP; n++) {
-        hx[i] = fma2(ops.Dr[i * NP + n], a[n], hx[i]);
-        hx[i] = fma2(ops.Ds[i * NP + n], b[n], hx[i]);
-        hz[i] = fma2(ops.Dr[i * NP + n], c[n], hz[i]);
-        hz[i] = fma2(ops.Ds[i * NP + n], d[n], hz[i]);
+        hx[i] = axpy_c(p2_dr(i * NP + n), a[n], hx[i]);
+        hz[i] = axpy_c(p2_dr(i * NP + n), c[n], hz[i]);
+        hx[i] = axpy_c(p2_ds(i * NP + n), b[n], hx[i]);
+        hz[i] = axpy_c(p2_ds(i * NP + n), d[n], hz[i]);
       }
   }
   float2 vx[NP], vz[NP], cx[NP], cz[NP];
@@ -564,10 +564,10 @@ __device__ __forceinline__ void stress_x2e_body(const Ops2& ops, const MeshDev<f
     float2 drx = f2(0.f), dsx = f2(0.f), drz = f2(0.f), dsz = f2(0.f);
 #pragma unroll
     for (int n = 0; n < NP; n++) {
-      drx = fma2(ops.Dr[i * NP + n], vx[n], drx);
-      dsx = fma2(ops.Ds[i * NP + n], vx[n], dsx);
-      drz = fma2(ops.Dr[i * NP + n], vz[n], drz);
-      dsz = fma2(ops.Ds[i * NP + n], vz[n], dsz);
+      drx = axpy_c(p2_dr(i * NP + n), vx[n], drx);
+      drz = axpy_c(p2_dr(i * NP + n), vz[n], drz);
+      dsx = axpy_c(p2_ds(i * NP + n), vx[n], dsx);
+      dsz = axpy_c(p2_ds(i * NP + n), vz[n], dsz);
     }
     X[i] = fma2(rx, drx, mul2(sx, dsx));
     Z[i] = fma2(rz, drz, mul2(sz, dsz));
@@ -601,10 +601,10 @@ __device__ __forceinline__ void stress_x2e_body(const Ops2& ops, const MeshDev<f
     for (int i = 0; i < NP; i++)
 #pragma unroll
       for (int k = 0; k < NF; k++) {
-        const float2 l = ops.L[(j * NP + i) * NF + k];
-        X[i] = fma2(l, fa[k], X[i]);
-        Z[i] = fma2(l, fb[k], Z[i]);
-        W[i] = fma2(l, fw[k], W[i]);
+        const float l = p2_lift((j * NP + i) * NF + k);
+        X[i] = axpy_c(l, fa[k], X[i]);
+        Z[i] = axpy_c(l, fb[k], Z[i]);
+        W[i] = axpy_c(l, fw[k], W[i]);
       }
   }
   const float4 m0 = __ldg(m.mat + e0), m1 = __ldg(m.mat + e1);

@@ -368,8 +368,13 @@ def run_ours(args):
         with eng.Engine(meshes, "fp64", device=device) as e64:
             e64.step(acc_steps)
             tr64 = traces(e64)
-        accuracy = {"trace_rel_l2_vs_fp64": float(np.linalg.norm(tr - tr64) / max(np.linalg.norm(tr64), 1e-300)),
-                    "steps": acc_steps, "shots": S_tot}
+        if np.linalg.norm(tr64) > 0:
+            accuracy = {"trace_rel_l2_vs_fp64": float(np.linalg.norm(tr - tr64) / np.linalg.norm(tr64)),
+                        "steps": acc_steps, "shots": S_tot}
+        else:  # the wave has not reached a receiver yet: nothing to compare
+            accuracy = {"trace_rel_l2_vs_fp64": None, "steps": acc_steps, "shots": S_tot,
+                        "note": "FP64 traces still zero after %d steps (source delay); the long-run "
+                                "accuracy of this workload is checked in tests/test_gpu_fullsize.py" % acc_steps}
 
     # ---- plain FP64 path on the first mesh: one shot, L2 flushed before every step ----------
     s1 = P.host.build_setup(one_shot(ws[0]), full=False, n_steps=table)

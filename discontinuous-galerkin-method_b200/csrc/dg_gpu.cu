@@ -114,6 +114,7 @@ struct dg_gpu_ctx {
   bool mx = false;  // FP32 batch of meshes: per-block dispatch to the packed bodies (k_*_mx)
   bool wave = false;  // one launch per step (k_step_wave), RCM order, chunk schedule in wv
   Wave wv{};
+  int stall_unit = -1, stall_saved = 0;  // wait-list entry replaced by dg_gpu_debug_stall_wave
   std::vector<int4> face_h;    // face codes of mesh 0 (internal numbering), for the chunk schedule
   std::vector<int> rec_elem_h; // receiver elements of mesh 0 (internal numbering)
   int num_sms = 148;
@@ -620,10 +621,12 @@ int build_wave(dg_gpu_ctx* c) {
   if ((rc = c->upload(&d_wait, wait))) return rc;
   if ((rc = c->upload(&d_rs, rstart))) return rc;
   if ((rc = c->upload(&d_rl, rlist))) return rc;
-  if ((rc = c->alloc(&d_flag, NU))) return rc;
+  // flag NU is never published: dg_gpu_debug_stall_wave points a wait at it
+  if ((rc = c->alloc(&d_flag, NU + 1))) return rc;
   if ((rc = c->alloc(&d_tk, 1))) return rc;
   if ((rc = c->alloc(&d_err, 1))) return rc;
-  CK(cudaMemsetAsync(d_flag, 0, sizeof(unsigned) * NU, c->stream));
+  CK(cudaMemsetAsync(d_flag, 0, sizeof(unsigned) * (NU + 1), c->stream));
+  c->stall_unit = -1;
   CK(cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
   Wave& w = c->wv;
   w.NU = NU;
@@ -841,7 +844,7 @@ int zero_state(dg_gpu_ctx* c) {
   }
   CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), c->stream));
   if (c->wave) {  // step ids restart at 1: clear the published flags and the tickets
-    CK(cudaMemsetAsync(c->wv.vflag, 0, sizeof(unsigned) * c->wv.NU, c->stream));
+    CK(cudaMemsetAsync(c->wv.vflag, 0, sizeof(unsigned) * (c->wv.NU + 1), c->stream));
     CK(cudaMemsetAsync(c->wv.tickets, 0, sizeof(unsigned long long), c->stream));
     CK(cudaMemsetAsync(c->wv.error, 0, sizeof(int), c->stream));
   }
@@ -1035,9 +1038,10 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   c->stage_elems = stage;
   CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), c->stream));
 
-  // automatic block size: 64 threads for the packed two-shot kernels (one or two elements per
-  // warp, so small blocks spread a chunk's neighbours over more SMs), 256 otherwise
-  int block = o.block_threads ? o.block_threads : (c->x2 >= 2 ? 64 : 256);
+  // automatic block size: 64 threads (measured 2-4 % ahead of 128 and 256 on every family of
+  // the time step: small blocks of these latency-bound kernels end and refill SMs sooner), 256
+  // for the reference-operator kernels
+  int block = o.block_threads ? o.block_threads : (o.precision == DG_FP64_REF ? 256 : 64);
   if ((rc = set_block(c.get(), block))) return rc;
   if (o.autotune && !o.block_threads)
     if ((rc = autotune(c.get(), o.tune_cache))) return rc;
@@ -1262,6 +1266,29 @@ int dg_gpu_reset(dg_gpu_ctx* c) {
   if (!c) return fail(DG_ERR_ARG, "null context");
   CK(cudaSetDevice(c->device));
   return zero_state(c);
+}
+
+int dg_gpu_debug_stall_wave(dg_gpu_ctx* c, int unit) {
+  if (!c) return fail(DG_ERR_ARG, "null context");
+  if (!c->wave) return fail(DG_ERR_UNSUPPORTED, "this context has no wavefront step");
+  if (unit >= c->wv.NU) return fail(DG_ERR_ARG, "unit out of range");
+  CK(cudaSetDevice(c->device));
+  int* slot = const_cast<int*>(c->wv.wait);
+  if (c->stall_unit >= 0) {  // put the replaced entry back
+    CK(cudaMemcpyAsync(slot + (size_t)c->stall_unit * c->wv.W, &c->stall_saved, sizeof(int),
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->stall_unit = -1;
+  }
+  if (unit >= 0) {
+    const int never = c->wv.NU;
+    CK(cudaMemcpyAsync(&c->stall_saved, slot + (size_t)unit * c->wv.W, sizeof(int), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaMemcpyAsync(slot + (size_t)unit * c->wv.W, &never, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->stall_unit = unit;
+  }
+  return DG_OK;
 }
 
 int dg_gpu_set_wavelet(dg_gpu_ctx* c, int mesh, long t0, long n, const double* w) {

@@ -35,7 +35,8 @@ def _ptr(a):
 EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_timed", "dg_gpu_step_profiled",
            "dg_gpu_fetch_traces", "dg_gpu_fetch", "dg_gpu_load",
            "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_steps_done",
-           "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error", "dg_gpu_energy_noalloc"]
+           "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error", "dg_gpu_energy_noalloc",
+           "dg_gpu_debug_stall_wave"]
 
 
 def energy_noalloc(device: int, K: int, fields, jacobi, A, inverV: np.ndarray, out, stream=None) -> None:
@@ -111,6 +112,7 @@ def lib(path: str | None = None):
         L.dg_gpu_reset.argtypes = [C.c_void_p]
         L.dg_gpu_set_wavelet.argtypes = [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p]
         L.dg_gpu_flush_l2.argtypes = [C.c_void_p]
+        L.dg_gpu_debug_stall_wave.argtypes = [C.c_void_p, C.c_int]
         L.dg_gpu_stats_get.argtypes = [C.c_void_p, C.c_void_p]
         L.dg_gpu_steps_done.argtypes = [C.c_void_p]
         L.dg_gpu_steps_done.restype = C.c_long
@@ -267,6 +269,11 @@ class Engine:
 
     def flush_l2(self):
         _check(lib().dg_gpu_flush_l2(self._ctx), "dg_gpu_flush_l2")
+
+    def debug_stall_wave(self, unit: int):
+        """Test hook: the stress update of warp unit `unit` of the wavefront step waits on a flag
+        that is never published (unit < 0 undoes it); the next step reports DG_ERR_TIMEOUT."""
+        _check(lib().dg_gpu_debug_stall_wave(self._ctx, int(unit)), "dg_gpu_debug_stall_wave")
 
     def stats(self) -> dict:
         s = _Stats()

@@ -133,7 +133,8 @@ int dg_gpu_step_timed(dg_gpu_ctx *ctx, long n);
 
 /* Advance n steps with a CUDA event before, between and after the two launches of every step,
  * all on the context stream and without host synchronisation until the end.  ms_vel / ms_str
- * (n floats each, may be NULL) receive each launch's device time; ms_total the time from the
+ * (n floats each, may be NULL) receive each launch's device time (the wavefront step is one
+ * launch: its time lands in ms_vel, ms_str holds about 0); ms_total the time from the
  * first event to the last.  With flush_l2 != 0 a buffer larger than L2 is written before every
  * step, outside the timed launches (ms_total then counts launches only). */
 int dg_gpu_step_profiled(dg_gpu_ctx *ctx, long n, int flush_l2, float *ms_vel, float *ms_str, double *ms_total);
@@ -159,6 +160,13 @@ int dg_gpu_set_wavelet(dg_gpu_ctx *ctx, int mesh, long t0, long n, const double 
 
 /* Write a buffer larger than L2 on the context stream (timing hygiene between measurements). */
 int dg_gpu_flush_l2(dg_gpu_ctx *ctx);
+
+/* Test hook of the wavefront step (no counterpart in the reference): unit >= 0 makes the stress
+ * update of that warp unit wait on a flag no warp ever publishes, so its wait reaches its limit
+ * (about a second) and the next dg_gpu_step returns DG_ERR_TIMEOUT, the state of that step being
+ * wrong; unit < 0 undoes it.  dg_gpu_reset then gives a context that steps as a fresh one.
+ * DG_ERR_UNSUPPORTED when the context has no wavefront step. */
+int dg_gpu_debug_stall_wave(dg_gpu_ctx *ctx, int unit);
 
 /* Largest mesh dg_gpu_energy_noalloc accepts: its scratch holds one partial sum per 256 elements. */
 #define DG_NOALLOC_MAX_ELEMENTS 4194304L

@@ -288,6 +288,33 @@ def test_wavefront_step_equals_two_pass_step(precision, S, block, margin, monkey
         assert np.array_equal(a, b)
 
 
+def test_wavefront_wait_limit_reports_timeout_and_context_recovers():
+    """A stress update made to wait on a flag that nothing publishes gives up after its limit:
+    the step returns DG_ERR_TIMEOUT instead of hanging, and after a reset the same context steps
+    exactly like a fresh one."""
+    g = Golden("square_3shots")
+    m, _ = _repeat_shots(g.setup_arrays(), 8)
+    with eng.Engine(m, "fp32", wavefront=1, block_threads=64) as fresh:
+        fresh.step(20)
+        want = [fresh.fetch(f, 0, s) for s in (0, 7) for f in FIELDS] + [fresh.fetch("trace_z", 0, 7)]
+    with eng.Engine(m, "fp32", wavefront=1, block_threads=64) as e:
+        e.step(2)
+        e.debug_stall_wave(5)
+        with pytest.raises(eng.DGError) as ei:
+            e.step(3)
+        assert ei.value.code == -10
+        e.debug_stall_wave(-1)
+        e.reset()
+        e.step(20)
+        got = [e.fetch(f, 0, s) for s in (0, 7) for f in FIELDS] + [e.fetch("trace_z", 0, 7)]
+    for a, b in zip(want, got):
+        assert np.array_equal(a, b)
+    with eng.Engine(m, "fp32", wavefront=-1) as e:
+        with pytest.raises(eng.DGError) as ei:
+            e.debug_stall_wave(0)
+        assert ei.value.code == -7
+
+
 def test_two_shot_and_one_shot_kernels_agree():
     g = Golden("slope_coupled")
     m, _ = _repeat_shots(g.setup_arrays(), 4, pattern=(0,))

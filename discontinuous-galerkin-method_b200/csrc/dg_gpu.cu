@@ -113,6 +113,8 @@ struct dg_gpu_ctx {
   int x2 = 0;
   bool mx = false;  // FP32 batch of meshes: per-block dispatch to the packed bodies (k_*_mx)
   bool wave = false;  // one launch per step (k_step_wave), RCM order, chunk schedule in wv
+  bool wave_persistent = false;  // k_step_wave_p: resident blocks looping over the tickets
+  int blocks_p = 0;              // its grid
   Wave wv{};
   int stall_unit = -1, stall_saved = 0;  // wait-list entry replaced by dg_gpu_debug_stall_wave
   std::vector<int4> face_h;    // face codes of mesh 0 (internal numbering), for the chunk schedule
@@ -563,8 +565,10 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
 // Schedule of the wavefront step for the current block size.  A unit is one warp's 32 threads of
 // the element range (thread g works on element g / H, H = shots / 2); the wait list holds, per unit, the
 // distinct units covering one of its elements or a neighbour of one; the lag L (in blocks) covers
-// the unit bandwidth plus a margin of about half the resident warps, so a stress update seldom
-// waits.  Receivers are listed under every unit that covers their element.
+// the unit bandwidth plus a margin of about 60 % of the resident warps, so a stress update
+// seldom waits.  Receivers are listed under every unit that covers their element.
+template <bool KAHAN> int wave_resident(dg_gpu_ctx* c, int& per_sm);
+
 int build_wave(dg_gpu_ctx* c) {
   const MeshHostInfo& h = c->mi[0];
   const long H = h.S_pad / 2;
@@ -616,6 +620,7 @@ int build_wave(dg_gpu_ctx* c) {
   int *d_wait, *d_rs, *d_rl;
   unsigned* d_flag;
   unsigned long long* d_tk;
+  unsigned* d_ptk;
   int* d_err;
   int rc;
   if ((rc = c->upload(&d_wait, wait))) return rc;
@@ -624,6 +629,8 @@ int build_wave(dg_gpu_ctx* c) {
   // flag NU is never published: dg_gpu_debug_stall_wave points a wait at it
   if ((rc = c->alloc(&d_flag, NU + 1))) return rc;
   if ((rc = c->alloc(&d_tk, 1))) return rc;
+  if ((rc = c->alloc(&d_ptk, 2))) return rc;
+  CK(cudaMemsetAsync(d_ptk, 0, sizeof(unsigned) * 2, c->stream));
   if ((rc = c->alloc(&d_err, 1))) return rc;
   CK(cudaMemsetAsync(d_flag, 0, sizeof(unsigned) * (NU + 1), c->stream));
   c->stall_unit = -1;
@@ -632,10 +639,11 @@ int build_wave(dg_gpu_ctx* c) {
   w.NU = NU;
   w.NB = NB;
   w.W = W;
-  // margin over the bandwidth, in blocks: about half the warps resident on the GPU, so that the
-  // velocity updates a stress update needs have mostly finished when it starts, while the lag
-  // window stays in L2 (DG_WAVE_MARGIN overrides it, for tuning)
-  int margin = (c->num_sms * 8 + WPB - 1) / WPB;
+  // margin over the bandwidth, in blocks: 10 warps per SM (about 60 % of the resident warps),
+  // so that the velocity updates a stress update needs have mostly finished when it starts,
+  // while the lag window stays in L2; measured flat from 1,200 to 1,800 warps on the 200k-element
+  // batch, much slower below 1,000 (DG_WAVE_MARGIN overrides it, in blocks, for tuning)
+  int margin = (c->num_sms * 10 + WPB - 1) / WPB;
   if (const char* env = getenv("DG_WAVE_MARGIN")) margin = std::max(0, atoi(env));
   w.L = Lb + margin;
   w.wait = d_wait;
@@ -643,11 +651,22 @@ int build_wave(dg_gpu_ctx* c) {
   w.rec_start = d_rs;
   w.rec_list = d_rl;
   w.tickets = d_tk;
+  w.ptk = d_ptk;
   w.error = d_err;
   w.spin_limit = 1u << 20;  // a million polls of an L2 line: well under a second
   c->blocks_v = NB + w.L;
   c->blocks_t = 0;
   w.inv_G = ~0ULL / (unsigned long long)c->blocks_v;
+  // persistent form for FP32 (6 % faster on the 200k x 64 batch); the Kahan body spills in it,
+  // so FP32_KAHAN keeps one block per ticket (DG_WAVE_PERSISTENT=0/1 overrides, for tuning)
+  c->wave_persistent = !c->kahan;
+  if (const char* env = getenv("DG_WAVE_PERSISTENT")) c->wave_persistent = atoi(env) != 0;
+  if (c->wave_persistent) {
+    int per_sm = 0;
+    if ((rc = c->kahan ? wave_resident<true>(c, per_sm) : wave_resident<false>(c, per_sm))) return rc;
+    if (per_sm < 1) return fail(DG_ERR_UNSUPPORTED, "the persistent wavefront kernel does not fit an SM");
+    c->blocks_p = std::min(c->blocks_v, per_sm * c->num_sms);
+  }
   k_wave_sync<<<1, 1, 0, c->stream>>>(c->d_ctr, d_tk, (unsigned)c->blocks_v);
   CK(cudaGetLastError());
   return DG_OK;
@@ -698,16 +717,35 @@ int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid) {
   return DG_OK;
 }
 
+// resident blocks of the persistent wavefront kernel for the current block size
+template <bool KAHAN>
+int wave_resident(dg_gpu_ctx* c, int& per_sm) {
+  cudaError_t e = cudaErrorInvalidValue;
+  per_sm = 0;
+  switch (c->x2) {
+#define DG_WO(SS) \
+  case SS: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_wave_p<SS, KAHAN>, c->block, 0); break;
+    DG_WO(2) DG_WO(4) DG_WO(8) DG_WO(16) DG_WO(32) DG_WO(64) DG_WO(128)
+#undef DG_WO
+    default: break;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __LINE__);
+  return DG_OK;
+}
+
 // shot counts with a wavefront step instance
 bool wave_supported(int S) { return S == 2 || S == 4 || S == 8 || S == 16 || S == 32 || S == 64 || S == 128; }
 
 template <bool KAHAN>
 int launch_wave(dg_gpu_ctx* c) {
-  const dim3 bl(c->block), g(c->blocks_v);
+  const dim3 bl(c->block), g(c->blocks_v), gp(c->blocks_p);
   switch (c->x2) {
-#define DG_WV(SS)                                                                           \
-  case SS:                                                                                  \
-    k_step_wave<SS, KAHAN><<<g, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr); \
+#define DG_WV(SS)                                                                                 \
+  case SS:                                                                                        \
+    if (c->wave_persistent)                                                                       \
+      k_step_wave_p<SS, KAHAN><<<gp, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr);   \
+    else                                                                                          \
+      k_step_wave<SS, KAHAN><<<g, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr);      \
     break;
     DG_WV(2) DG_WV(4) DG_WV(8) DG_WV(16) DG_WV(32) DG_WV(64) DG_WV(128)
 #undef DG_WV
@@ -846,6 +884,7 @@ int zero_state(dg_gpu_ctx* c) {
   if (c->wave) {  // step ids restart at 1: clear the published flags and the tickets
     CK(cudaMemsetAsync(c->wv.vflag, 0, sizeof(unsigned) * (c->wv.NU + 1), c->stream));
     CK(cudaMemsetAsync(c->wv.tickets, 0, sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(c->wv.ptk, 0, sizeof(unsigned) * 2, c->stream));
     CK(cudaMemsetAsync(c->wv.error, 0, sizeof(int), c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
@@ -1317,7 +1356,9 @@ int dg_gpu_stats_get(dg_gpu_ctx* c, dg_gpu_stats* out) {
   c->stats.block_threads = c->block;
   c->stats.graph_steps = c->graph_steps;
   c->stats.kernel_family =
-      c->precision == DG_FP64_REF ? 0 : (c->wave ? 5 : (c->mx ? 4 : (c->x2 == 1 ? 3 : (c->x2 ? 2 : 1))));
+      c->precision == DG_FP64_REF
+          ? 0
+          : (c->wave ? (c->wave_persistent ? 6 : 5) : (c->mx ? 4 : (c->x2 == 1 ? 3 : (c->x2 ? 2 : 1))));
   c->stats.bytes_per_step = c->wave ? c->bytes_wave : c->bytes_two_pass;
   *out = c->stats;
   return DG_OK;

@@ -42,6 +42,7 @@ struct Wave {
   int* error;             // bit 0: a wait reached its limit
   unsigned int spin_limit;
   unsigned long long inv_G;  // floor((2^64 - 1) / G), G = blocks of the launch
+  unsigned int* ptk;      // persistent form: [0] next ticket of the step, [1] blocks finished
 };
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -94,31 +95,11 @@ __global__ void k_wave_sync(const Counters* __restrict__ ctr, unsigned long long
   *tickets = (unsigned long long)ctr->v * G;
 }
 
+// The work of ticket tau in step t: the velocity half of the units of block tau and the stress
+// half of the units of block tau - L (each warp one unit of each).
 template <int S, bool KAHAN>
-__global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave(const __grid_constant__ Ops2 ops,
-                                                                 const __grid_constant__ MeshDev<float> m,
-                                                                 const __grid_constant__ Wave w,
-                                                                 Counters* __restrict__ ctr) {
-  __shared__ long long s_t;
-  __shared__ int s_tau;
-  if (threadIdx.x == 0) {
-    // the ticket gives both the step (ticket / G) and the block's place in it, so no block reads
-    // the counters and none has to rewind anything at the end of the launch; the quotient comes
-    // from the reciprocal, one short of the true one at most
-    const unsigned long long tk = atomicAdd(w.tickets, 1ull), G = gridDim.x;
-    unsigned long long q = __umul64hi(tk, w.inv_G);
-    if (tk - q * G >= G) q++;
-    s_t = (long long)q;
-    s_tau = (int)(tk - q * G);
-  }
-  __syncthreads();
-  const long long t = s_t;
-  const int tau = s_tau;
-  if (tau == 0 && threadIdx.x == 0) {
-    ctr->v = t + 1;
-    ctr->s = t + 1;
-  }
-  if (t >= m.steps) return;
+__device__ __forceinline__ void wave_ticket(const Ops2& ops, const MeshDev<float>& m, const Wave& w, int tau,
+                                            long long t) {
   const unsigned id = (unsigned)(t + 1);
   const int wpb = (int)(blockDim.x >> 5), warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
   const int uv = tau * wpb + warp, j = tau - w.L, ut = j * wpb + warp;
@@ -150,6 +131,74 @@ __global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave(const 
   if (do_t) {
     wait_units(w, k, id);
     if (g < m.K * H) stress_x2_core<S, KAHAN, true>(ops, m, e, q, sc);
+  }
+}
+
+template <int S, bool KAHAN>
+__global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave(const __grid_constant__ Ops2 ops,
+                                                                 const __grid_constant__ MeshDev<float> m,
+                                                                 const __grid_constant__ Wave w,
+                                                                 Counters* __restrict__ ctr) {
+  __shared__ long long s_t;
+  __shared__ int s_tau;
+  if (threadIdx.x == 0) {
+    // the ticket gives both the step (ticket / G) and the block's place in it, so no block reads
+    // the counters and none has to rewind anything at the end of the launch; the quotient comes
+    // from the reciprocal, one short of the true one at most
+    const unsigned long long tk = atomicAdd(w.tickets, 1ull), G = gridDim.x;
+    unsigned long long q = __umul64hi(tk, w.inv_G);
+    if (tk - q * G >= G) q++;
+    s_t = (long long)q;
+    s_tau = (int)(tk - q * G);
+  }
+  __syncthreads();
+  const long long t = s_t;
+  const int tau = s_tau;
+  if (tau == 0 && threadIdx.x == 0) {
+    ctr->v = t + 1;
+    ctr->s = t + 1;
+  }
+  if (t >= m.steps) return;
+  wave_ticket<S, KAHAN>(ops, m, w, tau, t);
+}
+
+// Persistent form: a grid of resident blocks, each taking tickets 0 .. G-1 of the step in turn
+// (w.ptk[0]) and asking for its next ticket while it works on the current one.  A block that
+// holds an unstarted ticket p is busy with a lower ticket whose stress half waits only on lower
+// tickets still, so the waits cannot form a cycle.  The last block to finish (w.ptk[1]) rewinds
+// the tickets and advances the step counters; every block reads the counters before it counts
+// itself finished, so none sees the new value.
+template <int S, bool KAHAN>
+__global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave_p(const __grid_constant__ Ops2 ops,
+                                                                   const __grid_constant__ MeshDev<float> m,
+                                                                   const __grid_constant__ Wave w,
+                                                                   Counters* __restrict__ ctr) {
+  __shared__ int s_tau[2];
+  const long long t = ctr->v;
+  const int G = w.NB + w.L;
+  if (t < m.steps) {
+    if (threadIdx.x == 0) s_tau[0] = (int)atomicAdd(w.ptk, 1u);
+    __syncthreads();
+    int cur = s_tau[0];
+    for (int it = 0; cur < G; it++) {
+      unsigned nxt = 0;
+      if (threadIdx.x == 0) nxt = atomicAdd(w.ptk, 1u);  // used only after this ticket's work
+      wave_ticket<S, KAHAN>(ops, m, w, cur, t);
+      if (threadIdx.x == 0) s_tau[(it + 1) & 1] = (int)nxt;
+      __syncthreads();
+      cur = s_tau[(it + 1) & 1];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(w.ptk + 1, 1u) == gridDim.x - 1) {
+      w.ptk[0] = 0u;
+      w.ptk[1] = 0u;
+      ctr->v = t + 1;
+      ctr->s = t + 1;
+      __threadfence();
+    }
   }
 }
 

@@ -114,7 +114,8 @@ typedef struct {
 	int kernel_family;     /* 0 reference operators, 1 one (element, shot) per thread,
 	                          2 two shots per thread (packed FP32x2), 3 two elements per thread (packed),
 	                          4 FP32 batch of meshes, each block running its mesh's packed body,
-	                          5 wavefront step (one launch per step, two shots per thread) */
+	                          5 wavefront step (one launch per step, two shots per thread, one block per ticket),
+	                          6 the same with resident blocks that loop over the tickets (FP32 default) */
 } dg_gpu_stats;
 
 void dg_gpu_default_opts(dg_gpu_opts *opts);

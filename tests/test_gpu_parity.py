@@ -266,13 +266,16 @@ def test_two_shot_kernels_against_reference(precision, S):
             assert rel_l2(e.fetch("Txz", 0, s), g.z["shot%d_final_Txz" % idx[s]]) <= 1e-3
 
 
+@pytest.mark.parametrize("persistent", ["0", "1"])
 @pytest.mark.parametrize("precision", ["fp32", "fp32_kahan"])
 @pytest.mark.parametrize("S,block,margin", [(8, 64, None), (2, 256, 0), (64, 128, 0), (128, 256, None),
                                             (16, 64, 3)])
-def test_wavefront_step_equals_two_pass_step(precision, S, block, margin, monkeypatch):
-    """One launch per step (k_step_wave, RCM order) gives the same bits as the two launches, for
-    warps covering many elements (2 shots), one element (64) and half an element (128), and with
-    no lag margin (every stress update waits on velocity updates still in flight)."""
+def test_wavefront_step_equals_two_pass_step(precision, S, block, margin, persistent, monkeypatch):
+    """One launch per step (k_step_wave / k_step_wave_p, RCM order) gives the same bits as the
+    two launches, for warps covering many elements (2 shots), one element (64) and half an
+    element (128), with no lag margin (every stress update waits on velocity updates still in
+    flight), one block per ticket and resident blocks looping over the tickets."""
+    monkeypatch.setenv("DG_WAVE_PERSISTENT", persistent)
     if margin is not None:
         monkeypatch.setenv("DG_WAVE_MARGIN", str(margin))
     g = Golden("square_3shots")
@@ -280,7 +283,7 @@ def test_wavefront_step_equals_two_pass_step(precision, S, block, margin, monkey
     out = []
     for wf in (-1, 1):
         with eng.Engine(m, precision, wavefront=wf, block_threads=block) as e:
-            assert e.stats()["kernel_family"] == (5 if wf == 1 else 2)
+            assert e.stats()["kernel_family"] == ((6 if persistent == "1" else 5) if wf == 1 else 2)
             e.step(g.steps)
             out.append([e.fetch(f, 0, s) for s in (0, S // 2, S - 1) for f in FIELDS] +
                        [e.fetch("trace_x", 0, s) for s in range(S)] + [e.fetch("trace_z", 0, S - 1)])

@@ -131,11 +131,24 @@ struct dg_gpu_ctx {
   int watchdog_every = 0;
   dg_gpu_stats stats{};
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // snapshot pipeline (dg_gpu_step_snapshots): two device slots and two pinned host slots, each
+  // holding Vx and Vz of one snapshot, a copy stream and per-slot events
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t snap_conv[2] = {nullptr, nullptr}, snap_copy[2] = {nullptr, nullptr};
+  double* snap_dev = nullptr;
+  double* snap_host = nullptr;
+  size_t snap_elems = 0;  // doubles per field and slot
 
   ~dg_gpu_ctx() {
     if (graph) cudaGraphExecDestroy(graph);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
+    for (int k = 0; k < 2; k++) {
+      if (snap_conv[k]) cudaEventDestroy(snap_conv[k]);
+      if (snap_copy[k]) cudaEventDestroy(snap_copy[k]);
+    }
+    if (snap_host) cudaFreeHost(snap_host);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     for (void* p : allocs) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -571,21 +584,26 @@ template <bool KAHAN> int wave_resident(dg_gpu_ctx* c, int& per_sm);
 
 int build_wave(dg_gpu_ctx* c) {
   const MeshHostInfo& h = c->mi[0];
-  const long H = h.S_pad / 2;
+  // two-shot layout: H = S/2 threads per element; one-shot layout: thread p owns elements 2p and
+  // 2p+1 of the Kp padded elements, so a warp covers 64 elements
+  const bool one = c->x2 == 1;
+  const long H = one ? 1 : h.S_pad / 2;
   if (c->block % 32) return fail(DG_ERR_UNSUPPORTED, "block size not a multiple of 32");
   const int WPB = c->block / 32;
-  const long NUl = (h.K * H + 31) / 32;
+  const long threads = one ? h.Kp / 2 : h.K * H;
+  const long NUl = (threads + 31) / 32;
   if (NUl >= (1L << 30)) return fail(DG_ERR_UNSUPPORTED, "too many warps for the wavefront step");
   const int NU = (int)NUl, NB = (NU + WPB - 1) / WPB;
-  auto first_unit = [&](long e) { return (int)(e * H / 32); };
-  auto last_unit = [&](long e) { return (int)(((e + 1) * H - 1) / 32); };
+  auto first_unit = [&](long e) { return (int)(one ? e / 64 : e * H / 32); };
+  auto last_unit = [&](long e) { return (int)(one ? e / 64 : ((e + 1) * H - 1) / 32); };
   std::vector<int> nstart(NU + 1, 0), nlist;
   nlist.reserve((size_t)NU * 6);
   int Lb = 0, W = 1;
   std::vector<int> tmp;
   for (int u = 0; u < NU; u++) {
-    tmp.clear();
-    const long e0 = (long)u * 32 / H, e1 = std::min<long>(h.K - 1, ((long)u * 32 + 31) / H);
+    tmp.assign(1, u);  // a unit of padding elements only still lists itself
+    const long e0 = one ? (long)u * 64 : (long)u * 32 / H;
+    const long e1 = std::min<long>(h.K - 1, one ? (long)u * 64 + 63 : ((long)u * 32 + 31) / H);
     for (long e = e0; e <= e1; e++) {
       const int4 f = c->face_h[e];
       const long els[4] = {e, f.x >= 0 ? f.x >> 4 : -1, f.y >= 0 ? f.y >> 4 : -1, f.z >= 0 ? f.z >> 4 : -1};
@@ -657,9 +675,10 @@ int build_wave(dg_gpu_ctx* c) {
   c->blocks_v = NB + w.L;
   c->blocks_t = 0;
   w.inv_G = ~0ULL / (unsigned long long)c->blocks_v;
-  // persistent form for FP32 (6 % faster on the 200k x 64 batch); the Kahan body spills in it,
-  // so FP32_KAHAN keeps one block per ticket (DG_WAVE_PERSISTENT=0/1 overrides, for tuning)
-  c->wave_persistent = !c->kahan;
+  // persistent form for FP32 on the two-shot layout (6 % faster on the 200k x 64 batch); the
+  // Kahan body spills in it and the one-shot layout runs slower in it, so those keep one block
+  // per ticket (DG_WAVE_PERSISTENT=0/1 overrides, for tuning)
+  c->wave_persistent = !c->kahan && c->x2 >= 2;
   if (const char* env = getenv("DG_WAVE_PERSISTENT")) c->wave_persistent = atoi(env) != 0;
   if (c->wave_persistent) {
     int per_sm = 0;
@@ -723,9 +742,11 @@ int wave_resident(dg_gpu_ctx* c, int& per_sm) {
   cudaError_t e = cudaErrorInvalidValue;
   per_sm = 0;
   switch (c->x2) {
-#define DG_WO(SS) \
-  case SS: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_wave_p<SS, KAHAN>, c->block, 0); break;
-    DG_WO(2) DG_WO(4) DG_WO(8) DG_WO(16) DG_WO(32) DG_WO(64) DG_WO(128)
+#define DG_WO(SS, LAYOUT) \
+  case SS: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_wave_p<LAYOUT, KAHAN>, c->block, 0); break;
+    DG_WO(1, WaveOneShot)
+    DG_WO(2, WaveTwoShots<2>) DG_WO(4, WaveTwoShots<4>) DG_WO(8, WaveTwoShots<8>) DG_WO(16, WaveTwoShots<16>)
+    DG_WO(32, WaveTwoShots<32>) DG_WO(64, WaveTwoShots<64>) DG_WO(128, WaveTwoShots<128>)
 #undef DG_WO
     default: break;
   }
@@ -740,14 +761,17 @@ template <bool KAHAN>
 int launch_wave(dg_gpu_ctx* c) {
   const dim3 bl(c->block), g(c->blocks_v), gp(c->blocks_p);
   switch (c->x2) {
-#define DG_WV(SS)                                                                                 \
+#define DG_WV(SS, LAYOUT)                                                                          \
   case SS:                                                                                        \
     if (c->wave_persistent)                                                                       \
-      k_step_wave_p<SS, KAHAN><<<gp, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr);   \
+      k_step_wave_p<LAYOUT, KAHAN><<<gp, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr); \
     else                                                                                          \
-      k_step_wave<SS, KAHAN><<<g, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr);      \
+      k_step_wave<LAYOUT, KAHAN><<<g, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr);  \
     break;
-    DG_WV(2) DG_WV(4) DG_WV(8) DG_WV(16) DG_WV(32) DG_WV(64) DG_WV(128)
+    DG_WV(1, WaveOneShot)
+#define DG_WV2(SS) DG_WV(SS, WaveTwoShots<SS>)
+    DG_WV2(2) DG_WV2(4) DG_WV2(8) DG_WV2(16) DG_WV2(32) DG_WV2(64) DG_WV2(128)
+#undef DG_WV2
 #undef DG_WV
     default:
       return fail(DG_ERR_UNSUPPORTED, "no wavefront step for this shot count");
@@ -1019,9 +1043,15 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
     if (o.variant == 2 && p.kind == 0)
       return fail(DG_ERR_UNSUPPORTED, "no packed FP32 kernel for this mesh (FP32 only; at most 128 shots)");
     // the wavefront step: one FP32 mesh on the two-shot kernels; automatic = on
-    c->wave = !c->multi && p.kind == 2 && wave_supported(p.S_pad) && o.wavefront != -1;
+    // automatic: from 16 shots on.  Below, a warp covers several elements and the scattered
+    // small gathers in RCM order cost more than the HBM traffic the step saves (200k elements:
+    // 2 shots 0.096 ms against 0.073 for two launches, 4 shots 0.103 against 0.091, 8 even,
+    // 16 shots 0.199 against 0.228; one shot on 2M elements 0.234 against 0.185)
+    c->wave = !c->multi && o.wavefront != -1 &&
+              ((p.kind == 2 && wave_supported(p.S_pad) && (p.S_pad >= 16 || o.wavefront == 1)) ||
+               (p.kind == 1 && o.wavefront == 1));
     if (o.wavefront == 1 && !c->wave)
-      return fail(DG_ERR_UNSUPPORTED, "the wavefront step needs one FP32 mesh with 2, 4, 8, ..., 128 shots");
+      return fail(DG_ERR_UNSUPPORTED, "the wavefront step needs one FP32 mesh with 1, 2, 4, 8, ..., 128 shots");
     int rc = prepare(meshes[k], o.precision, c->wave ? 2 : o.reorder, p);
     if (rc) return rc;
     MeshHostInfo& h = c->mi[k];
@@ -1093,10 +1123,9 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   return DG_OK;
 }
 
-static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
-  if (!c || n < 0) return fail(DG_ERR_ARG, "bad arguments");
-  if (c->t + n > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
-  CK(cudaSetDevice(c->device));
+// Enqueue n steps on the context stream (graphs where they fit; the watchdog, when on,
+// synchronises at its checks).  The caller synchronises.
+static int enqueue_steps(dg_gpu_ctx* c, long n, bool timed) {
   c->stats.launches = 0;
   if (timed) { c->stats.ms_velocity = 0; c->stats.ms_stress = 0; }
   long done = 0;
@@ -1144,6 +1173,15 @@ static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
       if (flag) return fail(DG_ERR_NONFINITE, "NaN or Inf in the velocity fields");
     }
   }
+  return DG_OK;
+}
+
+static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
+  if (!c || n < 0) return fail(DG_ERR_ARG, "bad arguments");
+  if (c->t + n > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
+  CK(cudaSetDevice(c->device));
+  int rc = enqueue_steps(c, n, timed);
+  if (rc) return rc;
   CK(cudaStreamSynchronize(c->stream));
   c->stats.steps_done = c->t;
   return check_wave(c);
@@ -1233,6 +1271,83 @@ int dg_gpu_fetch_traces(dg_gpu_ctx* c, int mesh, long t0, long n, double* dst_x,
   CK(cudaMemcpyAsync(dst_z, c->d_stage + per, per * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return DG_OK;
+}
+
+// Convert Vx and Vz of (mesh, shot) into the reference layout, as doubles, at dst (2 * K * 6).
+static int enqueue_velocity_fetch(dg_gpu_ctx* c, int mesh, int shot, double* dst) {
+  const MeshHostInfo& h = c->mi[mesh];
+  const long long n = h.K * 6;
+  const int B = 256, grid = (int)((n + B - 1) / B);
+  for (int f = 0; f < 2; f++) {
+    if (c->is_double)
+      k_fetch_field<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].U, f * 6, c->md_d[mesh].ES, c->md_d[mesh].PS,
+                                                       shot, h.d_new_of_old, (int)h.K, dst + f * n);
+    else
+      k_fetch_field<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].U, f * 6, c->md_f[mesh].ES, c->md_f[mesh].PS,
+                                                      shot, h.d_new_of_old, (int)h.K, dst + f * n);
+  }
+  CK(cudaGetLastError());
+  return DG_OK;
+}
+
+int dg_gpu_step_snapshots(dg_gpu_ctx* c, long n, long every, int mesh, int shot, dg_gpu_snapshot_fn fn,
+                          void* user) {
+  if (!c || !fn || every <= 0 || n < 0 || n % every || mesh < 0 || mesh >= (int)c->mi.size())
+    return fail(DG_ERR_ARG, "bad arguments");
+  const MeshHostInfo& h = c->mi[mesh];
+  if (shot < 0 || shot >= h.S) return fail(DG_ERR_ARG, "shot out of range");
+  if (c->t + n > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
+  CK(cudaSetDevice(c->device));
+  const size_t per = (size_t)h.K * 6;  // doubles per field
+  if (per > c->snap_elems) {            // (re)size the rings: 2 slots x (Vx, Vz)
+    if (c->snap_host) {
+      CK(cudaFreeHost(c->snap_host));
+      c->snap_host = nullptr;
+    }
+    int rc = c->alloc(&c->snap_dev, 4 * per);
+    if (rc) return rc;
+    void* hp = nullptr;
+    if (cudaMallocHost(&hp, 4 * per * sizeof(double)) != cudaSuccess) return fail(DG_ERR_NOMEM, "pinned snapshot ring");
+    c->snap_host = (double*)hp;
+    c->snap_elems = per;
+  }
+  if (!c->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+      CK(cudaEventCreateWithFlags(&c->snap_conv[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->snap_copy[k], cudaEventDisableTiming));
+    }
+  }
+  const long J = n / every;
+  const long t0 = c->t;
+  auto deliver = [&](long j) -> int {
+    const int slot = (int)(j & 1);
+    CK(cudaEventSynchronize(c->snap_copy[slot]));
+    const double* base = c->snap_host + (size_t)slot * 2 * c->snap_elems;
+    fn(user, t0 + (j + 1) * every, base, base + per);
+    return DG_OK;
+  };
+  int rc;
+  for (long j = 0; j < J; j++) {
+    const int slot = (int)(j & 1);
+    if ((rc = enqueue_steps(c, every, false))) return rc;
+    // the device slot is free once the copy of snapshot j - 2 has finished
+    if (j >= 2) CK(cudaStreamWaitEvent(c->stream, c->snap_copy[slot], 0));
+    double* dslot = c->snap_dev + (size_t)slot * 2 * c->snap_elems;
+    if ((rc = enqueue_velocity_fetch(c, mesh, shot, dslot))) return rc;
+    CK(cudaEventRecord(c->snap_conv[slot], c->stream));
+    CK(cudaStreamWaitEvent(c->copy_stream, c->snap_conv[slot], 0));
+    // the host slot is free: the callback of snapshot j - 2 returned before this loop turn
+    CK(cudaMemcpyAsync(c->snap_host + (size_t)slot * 2 * c->snap_elems, dslot, 2 * per * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->copy_stream));
+    CK(cudaEventRecord(c->snap_copy[slot], c->copy_stream));
+    // while the device works on snapshot j, hand snapshot j - 1 to the caller
+    if (j >= 1 && (rc = deliver(j - 1))) return rc;
+  }
+  if (J >= 1 && (rc = deliver(J - 1))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->stats.steps_done = c->t;
+  return check_wave(c);
 }
 
 int dg_gpu_fetch(dg_gpu_ctx* c, int what, int mesh, int shot, double* dst) {

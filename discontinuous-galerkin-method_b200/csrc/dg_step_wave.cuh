@@ -75,6 +75,69 @@ __device__ __forceinline__ void record_unit(const MeshDev<float>& m, const Wave&
   }
 }
 
+// Receivers of unit u of the one-shot layout (thread p owns elements 2p and 2p+1 of the
+// plane-major U[plane][Kp]): the thread that has just stored an element's velocities records it.
+__device__ __forceinline__ void record_unit_e(const MeshDev<float>& m, const Wave& w, int u, int r0, int r1,
+                                              long long t) {
+  const int p = u * 32 + (int)(threadIdx.x & 31);
+  float* tx = m.trace + (t * 2) * (long long)m.n_rec;
+  float* tz = tx + m.n_rec;
+  for (int q = r0; q < r1; q++) {
+    const int rr = __ldg(w.rec_list + q);
+    const int e = __ldg(m.rec_elem + rr);
+    if ((e >> 1) != p) continue;
+    const int node = __ldg(m.rec_node + rr);
+    tx[rr] = m.U[(long long)node * m.P + e];
+    tz[rr] = m.U[(long long)(6 + node) * m.P + e];
+  }
+}
+
+// Layouts of the wavefront step: how a block's velocity and stress halves, its receivers and
+// the stress half's early loads are done.
+template <int S>
+struct WaveTwoShots {  // element-major U[e][plane][S], thread g: element g / (S/2), shots 2q, 2q+1
+  using Pre = StressConst;
+  template <bool KAHAN>
+  static __device__ __forceinline__ void velocity(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
+    velocity_x2_body<S, KAHAN>(ops, m, lb, t);
+  }
+  static __device__ __forceinline__ void record(const MeshDev<float>& m, const Wave& w, int u, int r0, int r1,
+                                                long long t) {
+    record_unit<S>(m, w, u, r0, r1, t);
+  }
+  // the stress element's constants, requested before the release and the wait, which they
+  // overlap (a thread past the last element reads the last element's and discards them)
+  static __device__ __forceinline__ Pre prefetch(const MeshDev<float>& m, int lb) {
+    const int g = lb * (int)blockDim.x + (int)threadIdx.x;
+    return stress_const(m, min(g / (S / 2), m.K - 1));
+  }
+  template <bool KAHAN>
+  static __device__ __forceinline__ void stress(const Ops2& ops, const MeshDev<float>& m, int lb, long long t,
+                                                const Pre& sc) {
+    constexpr int H = S / 2;
+    const int g = lb * (int)blockDim.x + (int)threadIdx.x;
+    if (g < m.K * H) stress_x2_core<S, KAHAN, true>(ops, m, g / H, g - (g / H) * H, sc);
+  }
+};
+
+struct WaveOneShot {  // plane-major U[plane][Kp], thread p: elements 2p and 2p+1
+  struct Pre {};
+  template <bool KAHAN>
+  static __device__ __forceinline__ void velocity(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
+    velocity_x2e_body<KAHAN>(ops, m, lb, t);
+  }
+  static __device__ __forceinline__ void record(const MeshDev<float>& m, const Wave& w, int u, int r0, int r1,
+                                                long long t) {
+    record_unit_e(m, w, u, r0, r1, t);
+  }
+  static __device__ __forceinline__ Pre prefetch(const MeshDev<float>&, int) { return {}; }
+  template <bool KAHAN>
+  static __device__ __forceinline__ void stress(const Ops2& ops, const MeshDev<float>& m, int lb, long long t,
+                                                const Pre&) {
+    stress_x2e_body<KAHAN, true>(ops, m, lb, t);
+  }
+};
+
 // Each lane waits on one unit of the wait list (k < 0: none) to publish step id.
 __device__ __forceinline__ void wait_units(const Wave& w, int k, unsigned id) {
   if (k >= 0) {
@@ -97,7 +160,7 @@ __global__ void k_wave_sync(const Counters* __restrict__ ctr, unsigned long long
 
 // The work of ticket tau in step t: the velocity half of the units of block tau and the stress
 // half of the units of block tau - L (each warp one unit of each).
-template <int S, bool KAHAN>
+template <class Layout, bool KAHAN>
 __device__ __forceinline__ void wave_ticket(const Ops2& ops, const MeshDev<float>& m, const Wave& w, int tau,
                                             long long t) {
   const unsigned id = (unsigned)(t + 1);
@@ -114,27 +177,22 @@ __device__ __forceinline__ void wave_ticket(const Ops2& ops, const MeshDev<float
     r1 = __ldg(w.rec_start + uv + 1);
   }
   if (do_v) {
-    velocity_x2_body<S, KAHAN>(ops, m, tau, t);
+    Layout::template velocity<KAHAN>(ops, m, tau, t);
     __syncwarp();
-    if (r0 != r1) record_unit<S>(m, w, uv, r0, r1, t);
+    if (r0 != r1) Layout::record(m, w, uv, r0, r1, t);
     __syncwarp();
   }
-  // the stress element's constants are requested before the release and the wait, which they
-  // overlap (a thread past the last element reads the last element's and discards them)
-  constexpr int H = S / 2;
-  const int g = j * (int)blockDim.x + (int)threadIdx.x;
-  const int e = min(g / H, m.K - 1), q = g - (g / H) * H;
-  StressConst sc;
-  if (do_t) sc = stress_const(m, e);
+  typename Layout::Pre pre{};
+  if (do_t) pre = Layout::prefetch(m, j);
   // the warp barrier above orders every lane's stores before lane 0's release
   if (do_v && lane == 0) st_release_u32(w.vflag + uv, id);
   if (do_t) {
     wait_units(w, k, id);
-    if (g < m.K * H) stress_x2_core<S, KAHAN, true>(ops, m, e, q, sc);
+    Layout::template stress<KAHAN>(ops, m, j, t, pre);
   }
 }
 
-template <int S, bool KAHAN>
+template <class Layout, bool KAHAN>
 __global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave(const __grid_constant__ Ops2 ops,
                                                                  const __grid_constant__ MeshDev<float> m,
                                                                  const __grid_constant__ Wave w,
@@ -159,7 +217,7 @@ __global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave(const 
     ctr->s = t + 1;
   }
   if (t >= m.steps) return;
-  wave_ticket<S, KAHAN>(ops, m, w, tau, t);
+  wave_ticket<Layout, KAHAN>(ops, m, w, tau, t);
 }
 
 // Persistent form: a grid of resident blocks, each taking tickets 0 .. G-1 of the step in turn
@@ -168,7 +226,7 @@ __global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave(const 
 // tickets still, so the waits cannot form a cycle.  The last block to finish (w.ptk[1]) rewinds
 // the tickets and advances the step counters; every block reads the counters before it counts
 // itself finished, so none sees the new value.
-template <int S, bool KAHAN>
+template <class Layout, bool KAHAN>
 __global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave_p(const __grid_constant__ Ops2 ops,
                                                                    const __grid_constant__ MeshDev<float> m,
                                                                    const __grid_constant__ Wave w,
@@ -183,7 +241,7 @@ __global__ void __launch_bounds__(DG_WAVE_MAXT, DG_WAVE_MINB) k_step_wave_p(cons
     for (int it = 0; cur < G; it++) {
       unsigned nxt = 0;
       if (threadIdx.x == 0) nxt = atomicAdd(w.ptk, 1u);  // used only after this ticket's work
-      wave_ticket<S, KAHAN>(ops, m, w, cur, t);
+      wave_ticket<Layout, KAHAN>(ops, m, w, cur, t);
       if (threadIdx.x == 0) s_tau[(it + 1) & 1] = (int)nxt;
       __syncthreads();
       cur = s_tau[(it + 1) & 1];

@@ -399,10 +399,14 @@ __device__ __forceinline__ FaceLane face_lane(int code) {
   f.sponge = v && (code & 8);
   return f;
 }
+// FRESH: values other blocks of the same launch wrote (the wavefront step), read through L2
+template <bool FRESH = false>
 __device__ __forceinline__ float2 gather_pair(const MeshDev<float>& m, const FaceLane& a, const FaceLane& b, int pl,
                                               int k) {
-  return make_float2(m.U[(long long)(pl + a.node[k]) * m.P + a.nb] * a.mask,
-                     m.U[(long long)(pl + b.node[k]) * m.P + b.nb] * b.mask);
+  const float* pa = m.U + (long long)(pl + a.node[k]) * m.P + a.nb;
+  const float* pb = m.U + (long long)(pl + b.node[k]) * m.P + b.nb;
+  if (FRESH) return make_float2(__ldcg(pa) * a.mask, __ldcg(pb) * b.mask);
+  return make_float2(*pa * a.mask, *pb * b.mask);
 }
 
 template <bool KAHAN>
@@ -542,7 +546,7 @@ __global__ void __launch_bounds__(256, 2) k_velocity_x2e(const __grid_constant__
   velocity_x2e_body<KAHAN>(ops, m, blockIdx.x, t);
 }
 
-template <bool KAHAN>
+template <bool KAHAN, bool FRESH = false>
 __device__ __forceinline__ void stress_x2e_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
   const int p = lb * blockDim.x + threadIdx.x;
   const int H = m.Kp / 2;
@@ -552,7 +556,7 @@ __device__ __forceinline__ void stress_x2e_body(const Ops2& ops, const MeshDev<f
 
   float2 vx[NP], vz[NP];
 #pragma unroll
-  for (int i = 0; i < NP; i++) { vx[i] = Up[(0 + i) * H]; vz[i] = Up[(6 + i) * H]; }
+  for (int i = 0; i < NP; i++) { vx[i] = ld_v<FRESH>(Up + (0 + i) * H); vz[i] = ld_v<FRESH>(Up + (6 + i) * H); }
   const int4 f0 = __ldg(m.face + e0), f1 = __ldg(m.face + e1);
   const float4 g0 = __ldg(m.geo + e0), g1 = __ldg(m.geo + e1);
   const float2 rx = make_float2(g0.x, g1.x), sx = make_float2(g0.y, g1.y);
@@ -584,8 +588,8 @@ __device__ __forceinline__ void stress_x2e_body(const Ops2& ops, const MeshDev<f
     float2 px[NF], pz[NF];
 #pragma unroll
     for (int k = 0; k < NF; k++) {
-      px[k] = gather_pair(m, a, b, 0, k);
-      pz[k] = gather_pair(m, a, b, 6, k);
+      px[k] = gather_pair<FRESH>(m, a, b, 0, k);
+      pz[k] = gather_pair<FRESH>(m, a, b, 6, k);
     }
     float2 fa[NF], fb[NF], fw[NF];
 #pragma unroll

@@ -36,7 +36,7 @@ EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_tim
            "dg_gpu_fetch_traces", "dg_gpu_fetch", "dg_gpu_load",
            "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_steps_done",
            "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error", "dg_gpu_energy_noalloc",
-           "dg_gpu_debug_stall_wave"]
+           "dg_gpu_debug_stall_wave", "dg_gpu_step_snapshots"]
 
 
 def energy_noalloc(device: int, K: int, fields, jacobi, A, inverV: np.ndarray, out, stream=None) -> None:
@@ -94,6 +94,9 @@ KERNEL_NAMES = {0: ("k_velocity_ref", "k_stress_ref"), 1: ("k_velocity", "k_stre
 
 _LIB = None
 
+# void (*)(void *user, long step, const double *vx, const double *vz)
+SNAPSHOT_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_long, C.POINTER(C.c_double), C.POINTER(C.c_double))
+
 
 def lib(path: str | None = None):
     global _LIB
@@ -116,6 +119,9 @@ def lib(path: str | None = None):
         L.dg_gpu_set_wavelet.argtypes = [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_void_p]
         L.dg_gpu_flush_l2.argtypes = [C.c_void_p]
         L.dg_gpu_debug_stall_wave.argtypes = [C.c_void_p, C.c_int]
+        L.dg_gpu_step_snapshots.argtypes = [C.c_void_p, C.c_long, C.c_long, C.c_int, C.c_int, SNAPSHOT_FN,
+                                            C.c_void_p]
+        L.dg_gpu_step_snapshots.restype = C.c_int
         L.dg_gpu_stats_get.argtypes = [C.c_void_p, C.c_void_p]
         L.dg_gpu_steps_done.argtypes = [C.c_void_p]
         L.dg_gpu_steps_done.restype = C.c_long
@@ -224,6 +230,19 @@ class Engine:
         _check(lib().dg_gpu_step_profiled(self._ctx, int(n), 1 if flush_l2 else 0, mv.ctypes.data, ms.ctypes.data,
                                           C.byref(tot)), "dg_gpu_step_profiled")
         return mv[:n], ms[:n], tot.value
+
+    def step_snapshots(self, n: int, every: int, fn, mesh: int = 0, shot: int = 0):
+        """Advance n steps; after every `every` steps call fn(step, vx, vz) with copies of the
+        mesh/shot's Vx and Vz ([K][Np] doubles) while the device keeps stepping."""
+        K = self.info[mesh]["K"]
+
+        def cb(_user, step, vx, vz):
+            fn(int(step), np.ctypeslib.as_array(vx, shape=(K, 6)).copy(),
+               np.ctypeslib.as_array(vz, shape=(K, 6)).copy())
+
+        cfn = SNAPSHOT_FN(cb)
+        _check(lib().dg_gpu_step_snapshots(self._ctx, int(n), int(every), mesh, shot, cfn, None),
+               "dg_gpu_step_snapshots")
 
     def fetch_traces(self, t0: int, n: int, mesh: int = 0, out_x=None, out_z=None):
         """Traces of steps [t0, t0+n) of all shots, shape (shots, n, n_rec) each."""

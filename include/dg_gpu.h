@@ -99,7 +99,7 @@ typedef struct {
 	int variant;         /* FP32 kernels: 0 automatic, 1 one (element, shot) per thread,
 	                        2 packed FP32x2 kernels (two elements or two shots per thread) */
 	int wavefront;       /* one launch per step that keeps the state in flight in L2 (single FP32 mesh
-	                        with 2 or more shots): 0 automatic, 1 on, -1 off */
+	                        of 1, 2, 4, ..., 128 shots): 0 automatic (on from 16 shots), 1 on, -1 off */
 } dg_gpu_opts;
 
 typedef struct {
@@ -158,6 +158,20 @@ int dg_gpu_reset(dg_gpu_ctx *ctx);
 /* Replace wavelet samples [t0, t0+n) of one mesh with host values (the reference computes
  * w(t) on the host every step, DG_leap_Frog_OpenMP.c:421). */
 int dg_gpu_set_wavelet(dg_gpu_ctx *ctx, int mesh, long t0, long n, const double *w);
+
+/* Receives one velocity snapshot: step = steps done when it was taken, vx / vz = element-major
+ * [K][Np] doubles of the mesh and shot asked for (the layout of dg_gpu_fetch), valid only
+ * during the call. */
+typedef void (*dg_gpu_snapshot_fn)(void *user, long step, const double *vx, const double *vz);
+
+/* Advance n steps (a multiple of `every`) and hand Vx and Vz of (mesh, shot) to fn after every
+ * `every` steps, while the device keeps stepping: snapshot j is copied on a second stream into
+ * a pinned ring and fn(user, ...) runs on the calling thread while the device computes the
+ * steps after it.  Replaces the reference's Save_Data of Vx/Vz every 100 steps
+ * (DG_leap_Frog_OpenMP.c:433-444) without stalling the time loop; fn may write the files.
+ * Returns after the last call of fn and the last step. */
+int dg_gpu_step_snapshots(dg_gpu_ctx *ctx, long n, long every, int mesh, int shot, dg_gpu_snapshot_fn fn,
+                          void *user);
 
 /* Write a buffer larger than L2 on the context stream (timing hygiene between measurements). */
 int dg_gpu_flush_l2(dg_gpu_ctx *ctx);

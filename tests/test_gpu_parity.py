@@ -269,12 +269,13 @@ def test_two_shot_kernels_against_reference(precision, S):
 @pytest.mark.parametrize("persistent", ["0", "1"])
 @pytest.mark.parametrize("precision", ["fp32", "fp32_kahan"])
 @pytest.mark.parametrize("S,block,margin", [(8, 64, None), (2, 256, 0), (64, 128, 0), (128, 256, None),
-                                            (16, 64, 3)])
+                                            (16, 64, 3), (1, 64, None), (1, 128, 0)])
 def test_wavefront_step_equals_two_pass_step(precision, S, block, margin, persistent, monkeypatch):
     """One launch per step (k_step_wave / k_step_wave_p, RCM order) gives the same bits as the
-    two launches, for warps covering many elements (2 shots), one element (64) and half an
-    element (128), with no lag margin (every stress update waits on velocity updates still in
-    flight), one block per ticket and resident blocks looping over the tickets."""
+    two launches, for warps covering 64 elements (one shot, two elements per thread), many
+    elements (2 shots), one element (64) and half an element (128), with no lag margin (every
+    stress update waits on velocity updates still in flight), one block per ticket and resident
+    blocks looping over the tickets."""
     monkeypatch.setenv("DG_WAVE_PERSISTENT", persistent)
     if margin is not None:
         monkeypatch.setenv("DG_WAVE_MARGIN", str(margin))
@@ -283,7 +284,7 @@ def test_wavefront_step_equals_two_pass_step(precision, S, block, margin, persis
     out = []
     for wf in (-1, 1):
         with eng.Engine(m, precision, wavefront=wf, block_threads=block) as e:
-            assert e.stats()["kernel_family"] == ((6 if persistent == "1" else 5) if wf == 1 else 2)
+            assert e.stats()["kernel_family"] == ((6 if persistent == "1" else 5) if wf == 1 else (2 if S > 1 else 3))
             e.step(g.steps)
             out.append([e.fetch(f, 0, s) for s in (0, S // 2, S - 1) for f in FIELDS] +
                        [e.fetch("trace_x", 0, s) for s in range(S)] + [e.fetch("trace_z", 0, S - 1)])
@@ -316,6 +317,30 @@ def test_wavefront_wait_limit_reports_timeout_and_context_recovers():
         with pytest.raises(eng.DGError) as ei:
             e.debug_stall_wave(0)
         assert ei.value.code == -7
+
+
+@pytest.mark.parametrize("precision,S", [("fp64", 3), ("fp32", 16)])
+def test_snapshots_while_stepping_equal_step_then_fetch(precision, S):
+    """dg_gpu_step_snapshots hands over the same Vx/Vz as stepping `every` steps and fetching,
+    at the same steps, twice in a row (the rings are reused), and leaves the state where
+    dg_gpu_step would."""
+    g = Golden("square_3shots")
+    m, _ = _repeat_shots(g.setup_arrays(), S)
+    every, n = 15, 60  # 120 of the fixture's 150 steps
+    got = []
+    with eng.Engine(m, precision) as a, eng.Engine(m, precision) as b:
+        for _ in range(2):
+            a.step_snapshots(n, every, lambda step, vx, vz: got.append((step, vx, vz)), shot=S - 1)
+        want = []
+        for _ in range(2 * n // every):
+            b.step(every)
+            want.append((b.steps_done, b.fetch("Vx", 0, S - 1).reshape(-1, 6), b.fetch("Vz", 0, S - 1).reshape(-1, 6)))
+        assert a.steps_done == b.steps_done == 2 * n
+        assert np.array_equal(a.fetch("Txz", 0, 0), b.fetch("Txz", 0, 0))
+    assert [x[0] for x in got] == [x[0] for x in want] == list(range(every, 2 * n + 1, every))
+    for (_, vx, vz), (_, wx, wz) in zip(got, want):
+        assert np.array_equal(vx, wx) and np.array_equal(vz, wz)
+    assert np.any(got[-1][1])
 
 
 def test_two_shot_and_one_shot_kernels_agree():

@@ -308,6 +308,55 @@ static inline int outside_box(double x, double z, const dgh_setup_in *in)
 /* node number (1-based) of a triangle's corner slot: slot 0 -> 6, 1 -> 1, 2 -> 3 (fun_DG.c:329-340) */
 static const long corner_node[3] = {6, 1, 3};
 
+static const double *g_sort_x; /* positions being sorted by match_vertices (single-threaded use) */
+static int cmp_by_x(const void *a, const void *b)
+{
+	const double xa = g_sort_x[2 * *(const long *)a], xb = g_sort_x[2 * *(const long *)b];
+	return xa < xb ? -1 : (xa > xb ? 1 : (*(const long *)a < *(const long *)b ? -1 : 1));
+}
+static int cmp_long_pair(const void *a, const void *b)
+{
+	const long *x = a, *y = b;
+	return x[0] != y[0] ? (x[0] < y[0] ? -1 : 1) : (x[1] < y[1] ? -1 : (x[1] > y[1]));
+}
+
+/* For each of n query positions, the 1-based index of the first (last = 0) or last (last = 1)
+ * vertex whose coordinates both lie within tol of it, or -1: the matching rule of Get_Source /
+ * Get_Receiver, evaluated with one pass over the vertices. */
+static void match_vertices(const double *Point, long P, const double *pos, long n, double tol, int last, long *out)
+{
+	if (n <= 0) return;
+	long *ord = malloc(sizeof(long) * (size_t)n);
+	double *xs = malloc(sizeof(double) * (size_t)n);
+	for (long q = 0; q < n; q++) { out[q] = -1; if (ord) ord[q] = q; }
+	if (!ord || !xs) { /* out of memory: fall back to the direct scan */
+		for (long q = 0; q < n; q++)
+			for (long i = 0; i < P; i++)
+				if (fabs(Point[i * 2] - pos[q * 2]) < tol && fabs(Point[i * 2 + 1] - pos[q * 2 + 1]) < tol) {
+					out[q] = i + 1;
+					if (!last) break;
+				}
+		free(ord); free(xs);
+		return;
+	}
+	g_sort_x = pos;
+	qsort(ord, (size_t)n, sizeof(long), cmp_by_x);
+	for (long q = 0; q < n; q++) xs[q] = pos[2 * ord[q]];
+	for (long i = 0; i < P; i++) {
+		const double px = Point[i * 2], pz = Point[i * 2 + 1];
+		/* queries with x > px - tol - a margin (the exact test below decides) */
+		const double lo_x = px - 2 * tol;
+		long lo = 0, hi = n;
+		while (lo < hi) { const long mid = (lo + hi) / 2; if (xs[mid] < lo_x) lo = mid + 1; else hi = mid; }
+		for (long k = lo; k < n && xs[k] <= px + 2 * tol; k++) {
+			const long q = ord[k];
+			if (fabs(px - pos[q * 2]) < tol && fabs(pz - pos[q * 2 + 1]) < tol && (last || out[q] < 0)) out[q] = i + 1;
+		}
+	}
+	free(ord);
+	free(xs);
+}
+
 int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 {
 	if (!in || !out || in->K <= 0 || in->n_points <= 0 || !in->Point || !in->Triangle || !in->neighbor ||
@@ -397,18 +446,47 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 	if (out->wavelet)
 		for (long t = 0; t < in->n_steps; t++) out->wavelet[t] = dgh_ricker(t, out->dt, out->t0, in->fp, in->pi);
 
-	/* Get_Source + source vector (fun_DG.c:284-353; DG_leap_Frog_OpenMP.c:233-246) */
+	/* Get_Source + source vector (fun_DG.c:284-353; DG_leap_Frog_OpenMP.c:233-246): the first
+	 * vertex within 1e-3 and the first triangle holding it.  Get_Receiver (fun_DG.c:356-418):
+	 * the last vertex within 1e-2 and the last triangle holding it.  The reference scans all
+	 * vertices and triangles per source and receiver (O((S + R) K)); here one pass over the
+	 * vertices (binary search among the positions sorted by x) and one over the triangles give
+	 * the same indices. */
 	int rc = DGH_OK;
+	long *src_node = NULL, *rec_node = NULL, *src_tri = NULL, *rec_tri = NULL;
+	if (in->n_shots + in->n_rec > 0) {
+		const long S = in->n_shots, R = in->n_rec;
+		src_node = calloc((size_t)(S + R) * 4, sizeof(long));
+		if (!src_node) { rc = DGH_ERR_NOMEM; goto fail; }
+		rec_node = src_node + S;
+		src_tri = rec_node + R;  /* [S][2] triangle, slot */
+		rec_tri = src_tri + 2 * S; /* [R][2] */
+		match_vertices(in->Point, P, in->src_pos, S, 1e-3, 0, src_node);
+		match_vertices(in->Point, P, in->rec_pos, R, 1e-2, 1, rec_node);
+		for (long q = 0; q < 2 * (S + R); q++) src_tri[q] = -1;
+		/* vertex -> queries that matched it, as a sorted list of (vertex, query) pairs */
+		long nq = 0;
+		long *pairs = malloc(sizeof(long) * 2 * (size_t)(S + R));
+		if (!pairs) { rc = DGH_ERR_NOMEM; goto fail; }
+		for (long q = 0; q < S + R; q++)
+			if (src_node[q] > 0) { pairs[2 * nq] = src_node[q]; pairs[2 * nq + 1] = q; nq++; }
+		qsort(pairs, (size_t)nq, 2 * sizeof(long), cmp_long_pair);
+		for (long e = 0; e < K; e++)
+			for (int v = 0; v < 3; v++) {
+				const long node = in->Triangle[e * 3 + v];
+				long lo = 0, hi = nq;  /* first pair with vertex >= node */
+				while (lo < hi) { const long mid = (lo + hi) / 2; if (pairs[2 * mid] < node) lo = mid + 1; else hi = mid; }
+				for (long k = lo; k < nq && pairs[2 * k] == node; k++) {
+					const long q = pairs[2 * k + 1];
+					long *slot = q < S ? src_tri + 2 * q : rec_tri + 2 * (q - S);
+					if (q >= S || slot[0] < 0) { slot[0] = e + 1; slot[1] = corner_node[v]; }  /* sources: first */
+				}
+			}
+		free(pairs);
+	}
 	for (long m = 0; m < in->n_shots; m++) {
-		const double sx = in->src_pos[m * 2 + 0], sz = in->src_pos[m * 2 + 1];
-		long node = -1;
-		for (long i = 0; i < P; i++)
-			if (fabs(in->Point[i * 2 + 0] - sx) < 1e-3 && fabs(in->Point[i * 2 + 1] - sz) < 1e-3) { node = i + 1; break; }
-		if (node < 0) { rc = DGH_ERR_NOSOURCE; goto fail; }
-		long tri = -1, local = -1;
-		for (long e = 0; e < K && tri < 0; e++)
-			for (int v = 0; v < 3; v++)
-				if (in->Triangle[e * 3 + v] == node) { tri = e + 1; local = corner_node[v]; break; }
+		if (src_node[m] < 0) { rc = DGH_ERR_NOSOURCE; goto fail; }
+		const long tri = src_tri[2 * m], local = src_tri[2 * m + 1];
 		if (tri < 0) { rc = DGH_ERR_NOSOURCE; goto fail; }
 		if (out->source) { out->source[m * 2 + 0] = tri; out->source[m * 2 + 1] = local; }
 		if (out->fun) {
@@ -421,20 +499,14 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 		}
 	}
 
-	/* Get_Receiver (fun_DG.c:356-418): the last matching vertex, then the last triangle holding it */
 	for (long r = 0; r < in->n_rec; r++) {
-		const double rx = in->rec_pos[r * 2 + 0], rz = in->rec_pos[r * 2 + 1];
-		long node = -1;
-		for (long i = 0; i < P; i++)
-			if (fabs(in->Point[i * 2 + 0] - rx) < 1e-2 && fabs(in->Point[i * 2 + 1] - rz) < 1e-2) node = i + 1;
-		if (node < 0) { rc = DGH_ERR_NORECEIVER; goto fail; }
-		long tri = -1, local = -1;
-		for (long e = 0; e < K; e++)
-			for (int v = 0; v < 3; v++)
-				if (in->Triangle[e * 3 + v] == node) { tri = e + 1; local = corner_node[v]; }
+		if (rec_node[r] < 0) { rc = DGH_ERR_NORECEIVER; goto fail; }
+		const long tri = rec_tri[2 * r], local = rec_tri[2 * r + 1];
 		if (tri < 0) { rc = DGH_ERR_NORECEIVER; goto fail; }
 		if (out->receiver) { out->receiver[r * 2 + 0] = tri; out->receiver[r * 2 + 1] = local; }
 	}
+	free(src_node);
+	src_node = NULL;
 
 	/* Sponge: Get_Absorb_Square_Num, Get_absorb_square (vertex 0 only), Absorbing_Fun
 	 * (fun_DG.c:202-281, 879-1006) */
@@ -541,6 +613,7 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 	}
 
 fail:
+	free(src_node);
 	if (!out->Jacobi) free(Jac);
 	return rc;
 }

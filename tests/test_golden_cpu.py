@@ -114,3 +114,26 @@ def test_host_errors(bad, tmp_path):
         w.src = np.array([[123.456, 789.0]])
         with pytest.raises(host.HostError):
             host.build_setup(w)
+
+
+def test_source_and_receiver_vertex_rules_with_duplicate_vertices():
+    """Get_Source takes the FIRST vertex within 1e-3 of the position, Get_Receiver the LAST within
+    1e-2 (fun_DG.c:284-418).  A near-duplicate of a receiver vertex placed before every other
+    vertex (and used by no triangle) leaves the receivers as they were; a near-duplicate of the
+    source vertex there makes the source land on a vertex no triangle holds: NOSOURCE."""
+    w = pkg.workloads.small_square(n_cells=8, steps=5)
+    base = host.build_setup(w, full=False)
+    pts = host.quantize_e7(w.mesh.points)
+    tri = (w.mesh.tris + 1).astype(np.int64)
+    nb = np.where(w.mesh.neigh >= 0, w.mesh.neigh + 1, -1).astype(np.int64)
+
+    def with_duplicate(xz):
+        return (np.vstack([np.asarray(xz, dtype=np.float64)[None, :], pts]), tri + 1, nb)
+
+    r = w.rec[len(w.rec) // 2]
+    s = host.build_setup(w, full=False, mesh_arrays=with_duplicate([r[0] + 4e-3, r[1] - 4e-3]))
+    assert np.array_equal(s.arrays["receiver"], base.arrays["receiver"])
+    assert np.array_equal(s.arrays["source"], base.arrays["source"])
+    with pytest.raises(host.HostError) as ei:
+        host.build_setup(w, full=False, mesh_arrays=with_duplicate([w.src[0][0] + 5e-4, w.src[0][1]]))
+    assert "(-4)" in str(ei.value)

@@ -114,6 +114,7 @@ struct dg_gpu_ctx {
   bool mx = false;  // FP32 batch of meshes: per-block dispatch to the packed bodies (k_*_mx)
   bool wave = false;  // one launch per step (k_step_wave), RCM order, chunk schedule in wv
   bool wave_persistent = false;  // k_step_wave_p: resident blocks looping over the tickets
+  int margin_warps_per_sm = 10;  // lag margin of the wavefront step beyond the unit bandwidth
   int blocks_p = 0;              // its grid
   Wave wv{};
   int stall_unit = -1, stall_saved = 0;  // wait-list entry replaced by dg_gpu_debug_stall_wave
@@ -661,7 +662,7 @@ int build_wave(dg_gpu_ctx* c) {
   // so that the velocity updates a stress update needs have mostly finished when it starts,
   // while the lag window stays in L2; measured flat from 1,200 to 1,800 warps on the 200k-element
   // batch, much slower below 1,000 (DG_WAVE_MARGIN overrides it, in blocks, for tuning)
-  int margin = (c->num_sms * 10 + WPB - 1) / WPB;
+  int margin = (c->num_sms * c->margin_warps_per_sm + WPB - 1) / WPB;
   if (const char* env = getenv("DG_WAVE_MARGIN")) margin = std::max(0, atoi(env));
   w.L = Lb + margin;
   w.wait = d_wait;
@@ -675,11 +676,6 @@ int build_wave(dg_gpu_ctx* c) {
   c->blocks_v = NB + w.L;
   c->blocks_t = 0;
   w.inv_G = ~0ULL / (unsigned long long)c->blocks_v;
-  // persistent form for FP32 on the two-shot layout (6 % faster on the 200k x 64 batch); the
-  // Kahan body spills in it and the one-shot layout runs slower in it, so those keep one block
-  // per ticket (DG_WAVE_PERSISTENT=0/1 overrides, for tuning)
-  c->wave_persistent = !c->kahan && c->x2 >= 2;
-  if (const char* env = getenv("DG_WAVE_PERSISTENT")) c->wave_persistent = atoi(env) != 0;
   if (c->wave_persistent) {
     int per_sm = 0;
     if ((rc = c->kahan ? wave_resident<true>(c, per_sm) : wave_resident<false>(c, per_sm))) return rc;
@@ -916,30 +912,56 @@ int zero_state(dg_gpu_ctx* c) {
   return DG_OK;
 }
 
+// One schedule the autotuner can pick: threads per block and, for the wavefront step, one block
+// per ticket or resident blocks, and the lag margin in warps per SM.
+struct TuneChoice {
+  int block, persistent, margin;
+};
+
+int apply_choice(dg_gpu_ctx* c, const TuneChoice& t) {
+  if (c->wave) {
+    c->wave_persistent = t.persistent != 0;
+    c->margin_warps_per_sm = t.margin;
+  }
+  return set_block(c, t.block);
+}
+
+// Time each candidate schedule over a few steps from a zero state and keep the fastest; with a
+// cache file, reuse (and record) the choice for the same precision, mesh sizes and step form.
+// All candidates give the same results bit for bit; only the speed differs.
 int autotune(dg_gpu_ctx* c, const char* cache) {
   char key[256];
   long long sumK = 0, sumKS = 0;
   for (auto& h : c->mi) { sumK += h.K; sumKS += (long long)h.K * h.S; }
-  snprintf(key, sizeof key, "p%d_m%zu_K%lld_KS%lld", c->precision, c->mi.size(), sumK, sumKS);
+  snprintf(key, sizeof key, "p%d_m%zu_K%lld_KS%lld_w%d", c->precision, c->mi.size(), sumK, sumKS, c->wave ? 1 : 0);
   if (cache) {
     FILE* f = fopen(cache, "r");
     if (f) {
-      char k2[256];
-      int b;
-      while (fscanf(f, "%255s %d", k2, &b) == 2)
-        if (!strcmp(k2, key) && (b == 64 || b == 128 || b == 256)) {
+      char line[512], k2[256];
+      TuneChoice t{0, 0, 0};
+      while (fgets(line, sizeof line, f))
+        if (sscanf(line, "%255s %d %d %d", k2, &t.block, &t.persistent, &t.margin) == 4 && !strcmp(k2, key) &&
+            (t.block == 64 || t.block == 128 || t.block == 256) && t.margin > 0 && t.margin <= 64) {
           fclose(f);
-          return set_block(c, b);
+          return apply_choice(c, t);
         }
       fclose(f);
     }
   }
-  const int cand[3] = {64, 128, 256};
+  std::vector<TuneChoice> cand;
+  for (int b : {64, 128, 256}) {
+    if (!c->wave) {
+      cand.push_back({b, 0, c->margin_warps_per_sm});
+      continue;
+    }
+    for (int pers = 0; pers < 2; pers++)
+      for (int mw : {8, 10, 14}) cand.push_back({b, pers, mw});
+  }
   const long probe = std::min<long>(8, c->max_steps);
   float best = 1e30f;
-  int best_b = 256;
-  for (int b : cand) {
-    int rc = set_block(c, b);
+  TuneChoice best_t = cand[0];
+  for (const TuneChoice& t : cand) {
+    int rc = apply_choice(c, t);
     if (rc) return rc;
     for (int w = 0; w < 2 && w < probe; w++)
       if ((rc = launch_step(c))) return rc;
@@ -950,14 +972,15 @@ int autotune(dg_gpu_ctx* c, const char* cache) {
     CK(cudaEventSynchronize(c->ev[1]));
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
-    if (ms < best) { best = ms; best_b = b; }
+    if ((rc = check_wave(c))) return rc;
+    if (ms < best) { best = ms; best_t = t; }
     if ((rc = zero_state(c))) return rc;
   }
   if (cache) {
     FILE* f = fopen(cache, "a");
-    if (f) { fprintf(f, "%s %d\n", key, best_b); fclose(f); }
+    if (f) { fprintf(f, "%s %d %d %d\n", key, best_t.block, best_t.persistent, best_t.margin); fclose(f); }
   }
-  return set_block(c, best_b);
+  return apply_choice(c, best_t);
 }
 
 }  // namespace
@@ -1110,6 +1133,12 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   // automatic block size: 64 threads (measured 2-4 % ahead of 128 and 256 on every family of
   // the time step: small blocks of these latency-bound kernels end and refill SMs sooner), 256
   // for the reference-operator kernels
+  // persistent wavefront form for FP32 on the two-shot layout (6 % faster on the 200k x 64
+  // batch); the Kahan body spills in it and the one-shot layout runs slower in it, so those keep
+  // one block per ticket (DG_WAVE_PERSISTENT=0/1 overrides, for tuning)
+  c->wave_persistent = c->wave && !c->kahan && c->x2 >= 2;
+  if (const char* env = getenv("DG_WAVE_PERSISTENT"))
+    if (c->wave) c->wave_persistent = atoi(env) != 0;
   int block = o.block_threads ? o.block_threads : (o.precision == DG_FP64_REF ? 256 : 64);
   if ((rc = set_block(c.get(), block))) return rc;
   if (o.autotune && !o.block_threads)

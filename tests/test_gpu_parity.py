@@ -343,6 +343,27 @@ def test_snapshots_while_stepping_equal_step_then_fetch(precision, S):
     assert np.any(got[-1][1])
 
 
+@pytest.mark.parametrize("precision,S", [("fp32", 16), ("fp32_kahan", 16), ("fp64", 3)])
+def test_autotuned_schedule_gives_the_same_bits_and_is_cached(precision, S, tmp_path):
+    """The autotuner (block size; for the wavefront step also one block per ticket or resident
+    blocks, and the lag margin) changes speed only; a second context reads its choice back."""
+    g = Golden("square_3shots")
+    m, _ = _repeat_shots(g.setup_arrays(), S)
+    cache = str(tmp_path / "tune.txt")
+    out, stats = [], []
+    for kw in ({}, {"autotune": True, "tune_cache": cache}, {"autotune": True, "tune_cache": cache}):
+        with eng.Engine(m, precision, **kw) as e:
+            stats.append(e.stats())
+            e.step(g.steps)
+            out.append([e.fetch(f, 0, s) for s in (0, S - 1) for f in FIELDS] + [e.fetch("trace_z", 0, S - 1)])
+    for got in out[1:]:
+        for a, b in zip(out[0], got):
+            assert np.array_equal(a, b)
+    assert len(open(cache).read().splitlines()) == 1
+    assert stats[1]["block_threads"] == stats[2]["block_threads"]
+    assert stats[1]["kernel_family"] == stats[2]["kernel_family"]
+
+
 def test_two_shot_and_one_shot_kernels_agree():
     g = Golden("slope_coupled")
     m, _ = _repeat_shots(g.setup_arrays(), 4, pattern=(0,))

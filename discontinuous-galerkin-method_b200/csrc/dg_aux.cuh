@@ -18,6 +18,29 @@ __global__ void k_fetch_field(const R* __restrict__ U, int plane0, long long ES,
   out[q] = (double)U[(long long)en * ES + (plane0 + i) * PS + s];
 }
 
+// Halo exchange of a mesh split over several contexts: planes plane0 .. plane0+planes-1 of the
+// listed (internal) elements, all S shots, to or from buf[k][plane][s].
+template <class R>
+__global__ void k_halo_pack(const R* __restrict__ U, long long ES, long long PS, int S, int plane0, int planes,
+                            const int* __restrict__ elems, int n, R* __restrict__ buf) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)n * planes * S) return;
+  const int s = (int)(q % S);
+  const long long r = q / S;
+  const int pl = (int)(r % planes), k = (int)(r / planes);
+  buf[q] = U[(long long)__ldg(elems + k) * ES + (long long)(plane0 + pl) * PS + s];
+}
+template <class R>
+__global__ void k_halo_unpack(R* __restrict__ U, long long ES, long long PS, int S, int plane0, int planes,
+                              const int* __restrict__ elems, int n, const R* __restrict__ buf) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)n * planes * S) return;
+  const int s = (int)(q % S);
+  const long long r = q / S;
+  const int pl = (int)(r % planes), k = (int)(r / planes);
+  U[(long long)__ldg(elems + k) * ES + (long long)(plane0 + pl) * PS + s] = buf[q];
+}
+
 template <class R>
 __global__ void k_load_field(R* __restrict__ U, R* __restrict__ C, int plane0, long long ES, long long PS, int s,
                              const int* __restrict__ new_of_old, int K, const double* __restrict__ in) {

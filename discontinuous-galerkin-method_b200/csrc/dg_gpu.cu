@@ -118,6 +118,15 @@ struct dg_gpu_ctx {
   int blocks_p = 0;              // its grid
   Wave wv{};
   int stall_unit = -1, stall_saved = 0;  // wait-list entry replaced by dg_gpu_debug_stall_wave
+  // split meshes (dg_gpu_half_step / dg_gpu_halo_*): the velocity half of a step has run and its
+  // stress half has not; per mesh the internal elements sent to and received from other parts
+  bool half_pending = false;
+  struct Halo {
+    int* d_send = nullptr;
+    int* d_recv = nullptr;
+    long n_send = 0, n_recv = 0;
+  };
+  std::vector<Halo> halo;
   std::vector<int4> face_h;    // face codes of mesh 0 (internal numbering), for the chunk schedule
   std::vector<int> rec_elem_h; // receiver elements of mesh 0 (internal numbering)
   int num_sms = 148;
@@ -709,20 +718,20 @@ void choose_kind(int S, long K, bool fp32, int variant, int& kind, int& S_pad) {
 }
 
 template <bool KAHAN>
-int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid) {
+int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid, bool hv = true, bool ht = true) {
   const dim3 bl(c->block), gv(c->blocks_v), gt(c->blocks_t);
   cudaStream_t st = c->stream;
   switch (c->x2) {
     case 1:  // one shot: two elements per thread
-      k_velocity_x2e<KAHAN><<<gv, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);
+      if (hv) k_velocity_x2e<KAHAN><<<gv, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress_x2e<KAHAN><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);
+      if (ht) k_stress_x2e<KAHAN><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);
       break;
 #define DG_X2(SS)                                                                      \
   case SS:                                                                             \
-    k_velocity_x2<SS, KAHAN><<<gv, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);       \
+    if (hv) k_velocity_x2<SS, KAHAN><<<gv, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr); \
     if (mid) CK(cudaEventRecord(mid, st));                                             \
-    k_stress_x2<SS, KAHAN><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);         \
+    if (ht) k_stress_x2<SS, KAHAN><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);   \
     break;
     DG_X2(2) DG_X2(4) DG_X2(6) DG_X2(8) DG_X2(10) DG_X2(12) DG_X2(14) DG_X2(16) DG_X2(32) DG_X2(64) DG_X2(128)
 #undef DG_X2
@@ -775,30 +784,33 @@ int launch_wave(dg_gpu_ctx* c) {
   return DG_OK;
 }
 
-int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid = nullptr, cudaEvent_t after = nullptr) {
+// One step (halves = 3), or only its velocity (1) / stress (2) half for a split mesh.
+int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid = nullptr, cudaEvent_t after = nullptr,
+                int halves = 3) {
+  const bool hv = halves & 1, ht = halves & 2;
   const dim3 bl(c->block);
   const dim3 gv(c->blocks_v), gt(c->blocks_t);
   cudaStream_t st = c->stream;
   if (before_t) CK(cudaEventRecord(before_t, st));
   if (c->precision == DG_FP64_REF) {
     if (c->multi) {
-      k_velocity_ref<true><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
+      if (hv) k_velocity_ref<true><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress_ref<true><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
+      if (ht) k_stress_ref<true><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
     } else {
-      k_velocity_ref<false><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
+      if (hv) k_velocity_ref<false><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress_ref<false><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
+      if (ht) k_stress_ref<false><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
     }
   } else if (c->is_double) {
     if (c->multi) {
-      k_velocity<double, false, true><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
+      if (hv) k_velocity<double, false, true><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress<double, false, true><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
+      if (ht) k_stress<double, false, true><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
     } else {
-      k_velocity<double, false, false><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
+      if (hv) k_velocity<double, false, false><<<gv, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress<double, false, false><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
+      if (ht) k_stress<double, false, false><<<gt, bl, 0, st>>>(c->ops_d, c->md_d[0], nullptr, nullptr, c->d_ctr);
     }
   } else if (c->wave) {  // the whole step in one launch: it is timed as the "velocity" interval
     int rc = c->kahan ? launch_wave<true>(c) : launch_wave<false>(c);
@@ -806,36 +818,36 @@ int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid =
     if (mid) CK(cudaEventRecord(mid, st));
   } else if (c->mx) {
     if (c->kahan) {
-      k_velocity_mx<true><<<gv, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
+      if (hv) k_velocity_mx<true><<<gv, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress_mx<true><<<gt, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_t, c->d_ctr);
+      if (ht) k_stress_mx<true><<<gt, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_t, c->d_ctr);
     } else {
-      k_velocity_mx<false><<<gv, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
+      if (hv) k_velocity_mx<false><<<gv, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress_mx<false><<<gt, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_t, c->d_ctr);
+      if (ht) k_stress_mx<false><<<gt, bl, 0, st>>>(c->ops_f, c->ops2, c->d_tab_f, c->d_btab_t, c->d_ctr);
     }
   } else if (c->x2) {
-    int rc = c->kahan ? launch_x2<true>(c, mid) : launch_x2<false>(c, mid);
+    int rc = c->kahan ? launch_x2<true>(c, mid, hv, ht) : launch_x2<false>(c, mid, hv, ht);
     if (rc) return rc;
   } else if (c->kahan) {
     if (c->multi) {
-      k_velocity<float, true, true><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_ctr);
+      if (hv) k_velocity<float, true, true><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress<float, true, true><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_t, c->d_ctr);
+      if (ht) k_stress<float, true, true><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_t, c->d_ctr);
     } else {
-      k_velocity<float, true, false><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
+      if (hv) k_velocity<float, true, false><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress<float, true, false><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
+      if (ht) k_stress<float, true, false><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
     }
   } else {
     if (c->multi) {
-      k_velocity<float, false, true><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_ctr);
+      if (hv) k_velocity<float, false, true><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress<float, false, true><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_t, c->d_ctr);
+      if (ht) k_stress<float, false, true><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_t, c->d_ctr);
     } else {
-      k_velocity<float, false, false><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
+      if (hv) k_velocity<float, false, false><<<gv, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      k_stress<float, false, false><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
+      if (ht) k_stress<float, false, false><<<gt, bl, 0, st>>>(c->ops_f, c->md_f[0], nullptr, nullptr, c->d_ctr);
     }
   }
   CK(cudaGetLastError());
@@ -1207,6 +1219,7 @@ static int enqueue_steps(dg_gpu_ctx* c, long n, bool timed) {
 
 static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
   if (!c || n < 0) return fail(DG_ERR_ARG, "bad arguments");
+  if (c->half_pending) return fail(DG_ERR_STATE, "a velocity half step is waiting for its stress half");
   if (c->t + n > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
   CK(cudaSetDevice(c->device));
   int rc = enqueue_steps(c, n, timed);
@@ -1448,7 +1461,86 @@ int dg_gpu_load(dg_gpu_ctx* c, int what, int mesh, int shot, const double* src) 
 int dg_gpu_reset(dg_gpu_ctx* c) {
   if (!c) return fail(DG_ERR_ARG, "null context");
   CK(cudaSetDevice(c->device));
+  c->half_pending = false;
   return zero_state(c);
+}
+
+int dg_gpu_half_step(dg_gpu_ctx* c, int half) {
+  if (!c || (half != 0 && half != 1)) return fail(DG_ERR_ARG, "bad arguments");
+  if (c->wave) return fail(DG_ERR_UNSUPPORTED, "half steps need the two-launch step (wavefront = -1)");
+  if ((half == 0) == c->half_pending)
+    return fail(DG_ERR_STATE, half == 0 ? "velocity half again before the stress half" : "stress half without the velocity half");
+  if (half == 0 && c->t + 1 > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
+  CK(cudaSetDevice(c->device));
+  int rc = launch_step(c, nullptr, nullptr, nullptr, half == 0 ? 1 : 2);
+  if (rc) return rc;
+  c->half_pending = half == 0;
+  if (half == 1) {
+    c->t += 1;
+    c->stats.steps_done = c->t;
+  }
+  return DG_OK;
+}
+
+int dg_gpu_halo_lists(dg_gpu_ctx* c, int mesh, long n_send, const long* send, long n_recv, const long* recv) {
+  if (!c || mesh < 0 || mesh >= (int)c->mi.size() || n_send < 0 || n_recv < 0 || (n_send && !send) ||
+      (n_recv && !recv))
+    return fail(DG_ERR_ARG, "bad arguments");
+  const MeshHostInfo& h = c->mi[mesh];
+  std::vector<int> a(n_send), b(n_recv);
+  for (long k = 0; k < n_send; k++) {
+    if (send[k] < 0 || send[k] >= h.K) return fail(DG_ERR_ARG, "send element out of range");
+    a[k] = h.new_of_old[send[k]];
+  }
+  for (long k = 0; k < n_recv; k++) {
+    if (recv[k] < 0 || recv[k] >= h.K) return fail(DG_ERR_ARG, "receive element out of range");
+    b[k] = h.new_of_old[recv[k]];
+  }
+  CK(cudaSetDevice(c->device));
+  c->halo.resize(c->mi.size());
+  dg_gpu_ctx::Halo& hl = c->halo[mesh];
+  int rc;
+  if (n_send && (rc = c->upload(&hl.d_send, a))) return rc;
+  if (n_recv && (rc = c->upload(&hl.d_recv, b))) return rc;
+  hl.n_send = n_send;
+  hl.n_recv = n_recv;
+  CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
+// what 0: the velocity planes (Vx, Vz: 12), 1: the stress planes (Txx, Tzz, Txz: 18)
+static int halo_copy(dg_gpu_ctx* c, int mesh, int what, void* buf, bool pack) {
+  if (!c || mesh < 0 || mesh >= (int)c->mi.size() || (what != 0 && what != 1))
+    return fail(DG_ERR_ARG, "bad arguments");
+  if ((int)c->halo.size() <= mesh) return fail(DG_ERR_STATE, "no halo lists for this mesh");
+  const dg_gpu_ctx::Halo& hl = c->halo[mesh];
+  const long n = pack ? hl.n_send : hl.n_recv;
+  if (n == 0) return DG_OK;
+  if (!buf) return fail(DG_ERR_ARG, "null buffer");
+  const MeshHostInfo& h = c->mi[mesh];
+  const int plane0 = what == 0 ? 0 : 12, planes = what == 0 ? 12 : 18;
+  const long long total = (long long)n * planes * h.S;
+  const int B = 256;
+  const unsigned grid = (unsigned)((total + B - 1) / B);
+  CK(cudaSetDevice(c->device));
+  const int* el = pack ? hl.d_send : hl.d_recv;
+  if (c->is_double) {
+    const MeshDev<double>& m = c->md_d[mesh];
+    if (pack) k_halo_pack<double><<<grid, B, 0, c->stream>>>(m.U, m.ES, m.PS, h.S, plane0, planes, el, (int)n, (double*)buf);
+    else k_halo_unpack<double><<<grid, B, 0, c->stream>>>(m.U, m.ES, m.PS, h.S, plane0, planes, el, (int)n, (const double*)buf);
+  } else {
+    const MeshDev<float>& m = c->md_f[mesh];
+    if (pack) k_halo_pack<float><<<grid, B, 0, c->stream>>>(m.U, m.ES, m.PS, h.S, plane0, planes, el, (int)n, (float*)buf);
+    else k_halo_unpack<float><<<grid, B, 0, c->stream>>>(m.U, m.ES, m.PS, h.S, plane0, planes, el, (int)n, (const float*)buf);
+  }
+  CK(cudaGetLastError());
+  if (pack) CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
+int dg_gpu_halo_pack(dg_gpu_ctx* c, int mesh, int what, void* buf) { return halo_copy(c, mesh, what, buf, true); }
+int dg_gpu_halo_unpack(dg_gpu_ctx* c, int mesh, int what, const void* buf) {
+  return halo_copy(c, mesh, what, const_cast<void*>(buf), false);
 }
 
 int dg_gpu_debug_stall_wave(dg_gpu_ctx* c, int unit) {

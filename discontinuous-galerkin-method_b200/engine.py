@@ -36,7 +36,8 @@ EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_tim
            "dg_gpu_fetch_traces", "dg_gpu_fetch", "dg_gpu_load",
            "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_steps_done",
            "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error", "dg_gpu_energy_noalloc",
-           "dg_gpu_debug_stall_wave", "dg_gpu_step_snapshots"]
+           "dg_gpu_debug_stall_wave", "dg_gpu_step_snapshots", "dg_gpu_half_step", "dg_gpu_halo_lists",
+           "dg_gpu_halo_pack", "dg_gpu_halo_unpack"]
 
 
 def energy_noalloc(device: int, K: int, fields, jacobi, A, inverV: np.ndarray, out, stream=None) -> None:
@@ -122,6 +123,12 @@ def lib(path: str | None = None):
         L.dg_gpu_step_snapshots.argtypes = [C.c_void_p, C.c_long, C.c_long, C.c_int, C.c_int, SNAPSHOT_FN,
                                             C.c_void_p]
         L.dg_gpu_step_snapshots.restype = C.c_int
+        L.dg_gpu_half_step.argtypes = [C.c_void_p, C.c_int]
+        L.dg_gpu_halo_lists.argtypes = [C.c_void_p, C.c_int, C.c_long, C.c_void_p, C.c_long, C.c_void_p]
+        L.dg_gpu_halo_pack.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.dg_gpu_halo_unpack.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        for n in ("dg_gpu_half_step", "dg_gpu_halo_lists", "dg_gpu_halo_pack", "dg_gpu_halo_unpack"):
+            getattr(L, n).restype = C.c_int
         L.dg_gpu_stats_get.argtypes = [C.c_void_p, C.c_void_p]
         L.dg_gpu_steps_done.argtypes = [C.c_void_p]
         L.dg_gpu_steps_done.restype = C.c_long
@@ -243,6 +250,22 @@ class Engine:
         cfn = SNAPSHOT_FN(cb)
         _check(lib().dg_gpu_step_snapshots(self._ctx, int(n), int(every), mesh, shot, cfn, None),
                "dg_gpu_step_snapshots")
+
+    # ---- one part of a split mesh (decompose.SplitRun drives these) ----
+    def half_step(self, half: int):
+        _check(lib().dg_gpu_half_step(self._ctx, int(half)), "dg_gpu_half_step")
+
+    def halo_lists(self, send, recv, mesh: int = 0):
+        s = np.ascontiguousarray(send, dtype=np.int64)
+        r = np.ascontiguousarray(recv, dtype=np.int64)
+        _check(lib().dg_gpu_halo_lists(self._ctx, mesh, s.size, s.ctypes.data if s.size else None, r.size,
+                                       r.ctypes.data if r.size else None), "dg_gpu_halo_lists")
+
+    def halo_pack(self, what: int, dev_ptr: int, mesh: int = 0):
+        _check(lib().dg_gpu_halo_pack(self._ctx, mesh, int(what), C.c_void_p(dev_ptr)), "dg_gpu_halo_pack")
+
+    def halo_unpack(self, what: int, dev_ptr: int, mesh: int = 0):
+        _check(lib().dg_gpu_halo_unpack(self._ctx, mesh, int(what), C.c_void_p(dev_ptr)), "dg_gpu_halo_unpack")
 
     def fetch_traces(self, t0: int, n: int, mesh: int = 0, out_x=None, out_z=None):
         """Traces of steps [t0, t0+n) of all shots, shape (shots, n, n_rec) each."""

@@ -159,6 +159,40 @@ int dg_gpu_reset(dg_gpu_ctx *ctx);
  * w(t) on the host every step, DG_leap_Frog_OpenMP.c:421). */
 int dg_gpu_set_wavelet(dg_gpu_ctx *ctx, int mesh, long t0, long n, const double *w);
 
+/* ---- one mesh split over several contexts (one per GPU): domain decomposition --------------
+ * Replaces the reference's MPI driver (DG_leap_Frog_MPI.c:471-617), which keeps every array on
+ * every rank and all-gathers the stresses and then the velocities of all partition-boundary
+ * triangles twice per step (:486-558).  Here each context holds one part of the mesh: its own
+ * triangles plus ghost copies of the neighbouring triangles of other parts (faces of a ghost
+ * that lead out of the part are outer faces).  A step is
+ *     dg_gpu_half_step(ctx, 0)   velocity half (sponge, source, LU_Velocity) on every element
+ *     dg_gpu_halo_pack(ctx, m, 0, send) -> exchange -> dg_gpu_halo_unpack(ctx, m, 0, recv)
+ *     dg_gpu_half_step(ctx, 1)   stress half (LU_Stress_Elastic, Record), ends the step
+ *     dg_gpu_halo_pack(ctx, m, 1, send) -> exchange -> dg_gpu_halo_unpack(ctx, m, 1, recv)
+ * The ghosts' own updates are wrong (some neighbours are missing) but are overwritten by the
+ * exchange before any owned element reads them, so owned elements compute exactly what the whole
+ * mesh computes.  Receivers and sources belong to the part that owns their triangle.  Needs the
+ * two-launch step (opts.wavefront = -1). */
+
+/* Velocity half (half = 0) or stress half (half = 1) of the next step, enqueued on the context
+ * stream.  DG_ERR_STATE if the halves do not alternate; DG_ERR_UNSUPPORTED for a wavefront
+ * context. */
+int dg_gpu_half_step(dg_gpu_ctx *ctx, int half);
+
+/* Elements (0-based, the mesh's own numbering) whose values this part sends, and the ghost
+ * elements whose values it receives, each list in the order of the exchange buffers. */
+int dg_gpu_halo_lists(dg_gpu_ctx *ctx, int mesh, long n_send, const long *send, long n_recv, const long *recv);
+
+/* Copy the velocity (what = 0: Vx, Vz, 12 values per element and shot) or stress (what = 1:
+ * Txx, Tzz, Txz, 18 values) planes of the send list into the device buffer `buf`, laid out
+ * [element][plane][shot] in the context's arithmetic (8-byte doubles for the FP64 precisions,
+ * 4-byte floats for the FP32 ones); returns once the buffer is filled. */
+int dg_gpu_halo_pack(dg_gpu_ctx *ctx, int mesh, int what, void *buf);
+
+/* Copy a device buffer of the same layout into the planes of the receive list (enqueued on the
+ * context stream, ahead of the next half step). */
+int dg_gpu_halo_unpack(dg_gpu_ctx *ctx, int mesh, int what, const void *buf);
+
 /* Receives one velocity snapshot: step = steps done when it was taken, vx / vz = element-major
  * [K][Np] doubles of the mesh and shot asked for (the layout of dg_gpu_fetch), valid only
  * during the call. */

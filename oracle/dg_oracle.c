@@ -189,6 +189,44 @@ int dgo_run(const dgo_problem *p, long shot, long t_begin, long steps, double *V
 	return 0;
 }
 
+/*
+ * One half of step t, for the test of a mesh split into parts (the halves of dgo_run's step with
+ * an exchange of ghost values in between): half 0 = sponge on all fields, source, velocity
+ * update; half 1 = stress update and the record of step t into rec_x/rec_z[n_rec] (may be NULL).
+ */
+int dgo_half(const dgo_problem *p, long shot, long t, int half, double *Vx, double *Vz, double *Txx, double *Tzz,
+			 double *Txz, double *rec_x, double *rec_z)
+{
+	if (!p || !Vx || !Vz || !Txx || !Tzz || !Txz || t < 0 || t >= p->n_steps || (half != 0 && half != 1))
+		return -1;
+	const long K = p->K, KN = p->K * NP;
+	if (half == 0) {
+		const double w = p->wavelet[t];
+		for (long id = 0; id < KN; id++) {
+			const double a = p->absorb_fun[id];
+			Vx[id] *= a;
+			Vz[id] *= a;
+			Txx[id] *= a;
+			Tzz[id] *= a;
+			Txz[id] *= a;
+		}
+		for (int i = 0; i < NP; i++)
+			Vz[NP * (p->source[shot * 2 + 0] - 1) + i] += p->fun[shot * NP + i] * w;
+		for (long e = 0; e < K; e++)
+			velocity_element(p, e, Vx, Vz, Txx, Tzz, Txz);
+		return 0;
+	}
+	for (long e = 0; e < K; e++)
+		stress_element(p, e, Txx, Tzz, Txz, Vx, Vz);
+	if (rec_x && rec_z)
+		for (long r = 0; r < p->n_rec; r++) {
+			const long at = NP * (p->receiver[r * 2 + 0] - 1) + p->receiver[r * 2 + 1] - 1;
+			rec_x[r] = Vx[at];
+			rec_z[r] = Vz[at];
+		}
+	return 0;
+}
+
 int dgo_max_threads(void)
 {
 #ifdef _OPENMP

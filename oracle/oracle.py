@@ -42,6 +42,8 @@ def lib():
         _LIB.dgo_run.restype = C.c_int
         _LIB.dgo_run.argtypes = [C.c_void_p, C.c_long, C.c_long, C.c_long] + [C.c_void_p] * 7 + [C.c_int]
         _LIB.dgo_max_threads.restype = C.c_int
+        _LIB.dgo_half.restype = C.c_int
+        _LIB.dgo_half.argtypes = [C.c_void_p, C.c_long, C.c_long, C.c_int] + [C.c_void_p] * 7
     return _LIB
 
 
@@ -84,3 +86,13 @@ class Oracle:
             raise RuntimeError("oracle run failed (%d)" % rc)
         self.t += steps
         return rx, rz
+
+    def half(self, shot: int, t: int, half: int, rec_x=None, rec_z=None):
+        """One half of step t (0: sponge, source, velocity; 1: stress and record into the n_rec
+        arrays rec_x/rec_z), for the split-mesh test."""
+        if self.fields is None:
+            self.reset()
+        rc = lib().dgo_half(C.byref(self.prob), shot, t, half, *(a.ctypes.data for a in self.fields),
+                            None if rec_x is None else rec_x.ctypes.data, None if rec_z is None else rec_z.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("oracle half step failed (%d)" % rc)

@@ -9,6 +9,8 @@ module produces meshes of the same kind directly:
   vertices jittered by a seeded uniform offset (the homogeneous and layered configurations);
 * ``delaunay``        — a seeded Delaunay triangulation of jittered points clipped to a domain
   with a curved top (the slope/topography configurations);
+* ``read_poly`` / ``from_poly`` — a ``.poly`` planar straight-line graph (input_files/mesh/*.poly)
+  triangulated with its segments as mesh edges, regional attributes and holes;
 * ``write_converted`` — the ``.ele/.node/.neigh`` triple with the padded header row and the
   ``%16.7e`` MATLAB ``-ascii`` number format that ReadInt/ReadDouble parse
   (fun_save_to_file.c:22-204), 1-based indices, ``-1`` for "no neighbour".
@@ -216,6 +218,184 @@ def delaunay(width: float, height: float, h: float, *, seed: int = 0, jitter: fl
     cen = pts[tris].mean(axis=1)
     attr = np.ones(tris.shape[0], dtype=np.int64) if attr_fn is None else \
         np.asarray(attr_fn(cen[:, 0], cen[:, 1]), dtype=np.int64)
+    return Mesh(pts, tris, neigh, attr, _boundary_markers(pts.shape[0], tris, neigh))
+
+
+@dataclasses.dataclass
+class PSLG:
+    """A planar straight-line graph in Triangle's ``.poly`` terms."""
+
+    vertices: np.ndarray   # (V, 2) float64
+    segments: np.ndarray   # (E, 2) int64, 0-based vertex ids
+    holes: np.ndarray      # (H, 2) float64 seed points of holes
+    regions: np.ndarray    # (R, 4) float64: x, z, attribute, maximum triangle area (<= 0: none)
+
+
+def read_poly(src: str) -> PSLG:
+    """Parse a ``.poly`` file (a path or its text): vertex count/dim/attributes/markers, vertex
+    lines ``id x z [attributes] [marker]``, ``#segments [#markers]`` and ``id a b [marker]``,
+    ``#holes`` and ``id x z``, optionally ``#regions`` and ``id x z attribute max_area`` (the
+    inputs of input_files/mesh/*.poly).  Vertex ids may start at 0 or 1; ``#`` starts a comment."""
+    text = open(src).read() if os.path.exists(src) else src
+    rows = []
+    for line in text.splitlines():
+        line = line.split("#", 1)[0].strip()
+        if line:
+            rows.append(line.split())
+    nv = int(float(rows[0][0]))
+    at = 1
+    ids = []
+    verts = np.zeros((nv, 2))
+    for k in range(nv):
+        r = rows[at + k]
+        ids.append(int(float(r[0])))
+        verts[k] = float(r[1]), float(r[2])
+    at += nv
+    idx = {v: k for k, v in enumerate(ids)}
+    ne = int(float(rows[at][0]))
+    at += 1
+    segs = np.zeros((ne, 2), dtype=np.int64)
+    for k in range(ne):
+        r = rows[at + k]
+        segs[k] = idx[int(float(r[1]))], idx[int(float(r[2]))]
+    at += ne
+    holes = np.zeros((0, 2))
+    if at < len(rows):
+        nh = int(float(rows[at][0]))
+        at += 1
+        holes = np.array([[float(r[1]), float(r[2])] for r in rows[at:at + nh]]).reshape(-1, 2)
+        at += nh
+    regions = np.zeros((0, 4))
+    if at < len(rows):
+        nr = int(float(rows[at][0]))
+        at += 1
+        regions = np.array([[float(r[1]), float(r[2]), float(r[3]), float(r[4]) if len(r) > 4 else -1.0]
+                            for r in rows[at:at + nr]]).reshape(-1, 4)
+    return PSLG(verts, segs, holes, regions)
+
+
+def from_poly(pslg, h: float | None = None, *, seed: int = 0, jitter: float = 0.25, rotate: bool = True,
+              max_rounds: int = 30) -> Mesh:
+    """Triangulate a PSLG (what ``triangle -pqanA`` does for the reference, create_mesh_file.m:5):
+    triangles whose edges follow every segment, regional attributes, holes removed.
+
+    Points go along every segment (spacing <= h) and on a jittered offset-row lattice of spacing
+    h inside; lattice points within a sub-segment's diametral circle are dropped, so every
+    sub-segment is a Delaunay edge; a sub-segment that still is not (another segment's points
+    encroach on it) is split at its midpoint and the points are triangulated again.  Triangles
+    reachable from the convex hull or a hole seed without crossing a segment are removed; each
+    region seed's attribute fills the triangles reachable from it.  ``h`` defaults to the edge
+    of an equilateral triangle of the smallest regional maximum area (or 1/40 of the extent).
+    """
+    from scipy.spatial import Delaunay, cKDTree  # set-up time only
+
+    g = read_poly(pslg) if isinstance(pslg, str) else pslg
+    rng = np.random.default_rng(seed)
+    lo, hi = g.vertices.min(0), g.vertices.max(0)
+    if h is None:
+        areas = g.regions[:, 3][g.regions[:, 3] > 0] if g.regions.size else np.zeros(0)
+        h = float(np.sqrt(4.0 * areas.min() / np.sqrt(3.0))) if areas.size else float((hi - lo).max() / 40.0)
+    # sub-segments: consecutive points along each segment
+    sub = []        # list of (point a, point b) coordinate pairs
+    for a, b in g.segments:
+        pa, pb = g.vertices[a], g.vertices[b]
+        n = max(1, int(np.ceil(np.linalg.norm(pb - pa) / h - 1e-9)))
+        t = np.linspace(0.0, 1.0, n + 1)
+        pts = pa[None, :] + t[:, None] * (pb - pa)[None, :]
+        sub.extend(zip(pts[:-1], pts[1:]))
+    # interior lattice
+    hz = h * np.sqrt(3.0) / 2.0
+    rows = []
+    j = 0
+    while lo[1] + j * hz <= hi[1]:
+        off = 0.5 * h if j % 2 else 0.0
+        xr = np.arange(lo[0] + off, hi[0] + 1e-9, h)
+        rows.append(np.stack([xr, np.full_like(xr, lo[1] + j * hz)], 1))
+        j += 1
+    inner = np.concatenate(rows, 0)
+    inner = inner + rng.uniform(-jitter * h, jitter * h, size=inner.shape)
+
+    def key(p):
+        return (round(float(p[0]), 9), round(float(p[1]), 9))
+
+    for _ in range(max_rounds):
+        seg_pts = {}
+        for a, b in sub:
+            seg_pts.setdefault(key(a), a)
+            seg_pts.setdefault(key(b), b)
+        sp = np.array(list(seg_pts.values()))
+        mids = np.array([(a + b) / 2 for a, b in sub])
+        rad = np.array([np.linalg.norm(b - a) / 2 for a, b in sub])
+        # keep lattice points outside every diametral circle and away from segment points
+        keep = cKDTree(sp).query(inner)[0] > 0.45 * h
+        tree = cKDTree(inner)
+        for m, r in zip(mids, rad):
+            for i in tree.query_ball_point(m, r * 1.05):
+                keep[i] = False
+        pts = np.concatenate([sp, inner[keep]], 0)
+        tri = Delaunay(pts)
+        simp = tri.simplices.astype(np.int64)
+        edges = set()
+        for t in simp:
+            for u, v in ((t[0], t[1]), (t[1], t[2]), (t[2], t[0])):
+                edges.add((min(u, v), max(u, v)))
+        pid = {key(p): i for i, p in enumerate(pts)}
+        missing = []
+        for k, (a, b) in enumerate(sub):
+            u, v = pid[key(a)], pid[key(b)]
+            if (min(u, v), max(u, v)) not in edges:
+                missing.append(k)
+        if not missing:
+            break
+        for k in sorted(missing, reverse=True):
+            a, b = sub[k]
+            m = (a + b) / 2
+            sub[k:k + 1] = [(a, m), (m, b)]
+    else:
+        raise RuntimeError("could not make every segment a mesh edge")
+    # barrier edges, then flood fills over the triangle adjacency
+    barrier = set()
+    for a, b in sub:
+        u, v = pid[key(a)], pid[key(b)]
+        barrier.add((min(u, v), max(u, v)))
+    nbr = tri.neighbors.astype(np.int64)   # scipy: neighbour k lies opposite vertex k
+
+    def edge_of(t, k):
+        u, v = simp[t, (k + 1) % 3], simp[t, (k + 2) % 3]
+        return (min(u, v), max(u, v))
+
+    def fill(starts, mark, value):
+        stack = [s for s in starts if s >= 0 and mark[s] != value]
+        for s in stack:
+            mark[s] = value
+        while stack:
+            t = stack.pop()
+            for k in range(3):
+                n = nbr[t, k]
+                if n >= 0 and mark[n] != value and edge_of(t, k) not in barrier:
+                    mark[n] = value
+                    stack.append(n)
+
+    T = simp.shape[0]
+    outside = np.zeros(T, dtype=np.int64)
+    hull = [t for t in range(T) for k in range(3) if nbr[t, k] < 0 and edge_of(t, k) not in barrier]
+    fill(hull, outside, 1)
+    if g.holes.size:
+        fill(list(tri.find_simplex(g.holes)), outside, 1)
+    attr = np.zeros(T, dtype=np.int64)
+    for x, z, a, _area in g.regions:
+        fill([int(tri.find_simplex(np.array([[x, z]]))[0])], attr, int(round(a)))
+    inside = outside == 0
+    tris = simp[inside]
+    attr = attr[inside]
+    used = np.unique(tris)
+    remap = np.full(pts.shape[0], -1, dtype=np.int64)
+    remap[used] = np.arange(used.size)
+    pts = pts[used]
+    tris = remap[tris]
+    tris = _orient_ccw(pts, tris)
+    tris = _rotate(tris, rng if rotate else None)
+    neigh = compute_neighbors(tris)
     return Mesh(pts, tris, neigh, attr, _boundary_markers(pts.shape[0], tris, neigh))
 
 

@@ -51,6 +51,29 @@ def gardner(vp):
     return 310.0 * np.asarray(vp, dtype=np.float64) ** 0.25
 
 
+def poly_model(poly, materials: dict, src, rec, *, h=None, fp=15.0, sponge=None, steps=2000, seed=0) -> Workload:
+    """A model from a ``.poly`` planar straight-line graph (path or text; input_files/mesh/*.poly
+    are of this kind): triangulated by ``meshgen.from_poly``, region attribute ``a`` getting
+    ``materials[a] = (vp, vs, rho)`` (vs = 0: fluid), sources and receivers moved to the nearest
+    vertex.  ``sponge`` = (bound_x, bound_z, model_w, model_h) in absolute coordinates (dg.h:8-12);
+    default: a band of 5 % of the extent inside the bounding box.  The reference assigns
+    materials from the attributes in its driver (DG_leap_Frog_OpenMP.c:248-262)."""
+    mesh = meshgen.from_poly(poly, h, seed=seed)
+    table = {int(k): v for k, v in materials.items()}
+    missing = sorted(set(np.unique(mesh.attr).tolist()) - set(table))
+    if missing:
+        raise ValueError("no material for region attributes %s" % missing)
+    mat = np.array([table[int(a)] for a in mesh.attr], dtype=np.float64)
+    if sponge is None:
+        lo, hi = mesh.points.min(0), mesh.points.max(0)
+        b = 0.05 * (hi - lo)
+        sponge = (lo[0] + b[0], lo[1] + b[1], hi[0] - lo[0] - 2 * b[0], hi[1] - lo[1] - 2 * b[1])
+    if sponge[0] <= 0 or sponge[1] <= 0:
+        raise ValueError("the sponge box must start at positive coordinates (bound_x, bound_z > 0)")
+    return Workload("poly_model_K%d" % mesh.K, mesh, mat[:, 0], mat[:, 1], mat[:, 2], float(fp), tuple(sponge),
+                    meshgen.snap_to_vertices(mesh, src), meshgen.snap_to_vertices(mesh, rec), int(steps))
+
+
 def homogeneous_square(n_cells=100, size=2000.0, steps=2000, seed=0, n_rec=101, shots=1) -> Workload:
     """2 km x 2 km square, n x n cells split in two, interior vertices jittered +-10% h."""
     centre = (size / 2, size / 2)

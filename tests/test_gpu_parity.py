@@ -406,3 +406,23 @@ def test_two_shot_checkpoint_restore():
             for f in FIELDS:
                 assert np.array_equal(a.fetch(f, 0, s), b.fetch(f, 0, s))
             assert np.array_equal(a.fetch("trace_x", 0, s)[80:], b.fetch("trace_x", 0, s)[80:])
+
+
+def test_poly_model_against_oracle():
+    """A model meshed from a planar straight-line graph (two regions, acoustic over elastic)."""
+    from test_poly_mesh_cpu import L_SHAPE
+    w = pkg.workloads.poly_model(L_SHAPE, {1: (4000.0, 2300.0, 2500.0), 2: (1500.0, 0.0, 1000.0)},
+                                 src=[(1500.0, 500.0)], rec=[(x, 2400.0) for x in (100.0, 800.0, 1600.0)],
+                                 h=120.0, fp=8.0, steps=400)
+    s = pkg.host.build_setup(w, full=True)
+    o = oracle.Oracle.from_setup(s)
+    rx, rz = o.run(0, w.steps, threads=0)
+    with eng.Engine(eng.mesh_from_setup(s), "fp64_ref") as e:
+        e.step(w.steps)
+        assert np.array_equal(e.fetch("trace_z"), rz)
+        assert np.array_equal(e.fetch("Txz"), o.fields[4])
+    with eng.Engine(eng.mesh_from_setup(s), "fp64") as e:
+        e.step(w.steps)
+        assert rel_l2(np.concatenate([e.fetch("trace_x").ravel(), e.fetch("trace_z").ravel()]),
+                      np.concatenate([rx.ravel(), rz.ravel()])) <= 1e-10
+    assert np.abs(rz).max() > 0

@@ -1,10 +1,14 @@
 // dg_gpu.cu — host side of the sm_100a DG engine: the C ABI of include/dg_gpu.h.
 //
-// dg_gpu_init validates the reference's set-up arrays, renumbers elements along a Hilbert curve
-// of their centroids, converts the index maps into compact face codes and the per-element
-// operators into geometric factors (or keeps the reference's own operators for DG_FP64_REF),
-// and uploads everything.  dg_gpu_step replays a CUDA graph of `graph_steps` steps, each step
-// being one velocity and one stress launch (the stress launch also records the receivers).
+// dg_gpu_init validates the reference's set-up arrays, renumbers elements (along a Hilbert curve
+// of their centroids, or in reverse Cuthill-McKee order for the wavefront step), converts the
+// index maps into compact face codes and the per-element operators into geometric factors (or
+// keeps the reference's own operators for DG_FP64_REF), chooses the kernel family and block
+// size, builds the wavefront schedule where it applies, and uploads everything.  dg_gpu_step
+// replays a CUDA graph of `graph_steps` steps; a step is one velocity and one stress launch (the
+// stress launch also records the receivers) or one wavefront launch.  Further entry points:
+// snapshots overlapped with stepping, half steps and halo copies for a mesh split over several
+// contexts, the autotuner, checkpoint load/fetch, and the test hook of the wavefront waits.
 #include "dg_gpu.h"
 #include "dg_aux.cuh"
 #include "dg_common.cuh"
@@ -112,7 +116,7 @@ struct dg_gpu_ctx {
   // layout); S >= 2 two shots per thread (element-major layout U[e][plane][S])
   int x2 = 0;
   bool mx = false;  // FP32 batch of meshes: per-block dispatch to the packed bodies (k_*_mx)
-  bool wave = false;  // one launch per step (k_step_wave), RCM order, chunk schedule in wv
+  bool wave = false;  // one launch per step (k_step_wave / k_step_wave_p), RCM order, schedule in wv
   bool wave_persistent = false;  // k_step_wave_p: resident blocks looping over the tickets
   int margin_warps_per_sm = 10;  // lag margin of the wavefront step beyond the unit bandwidth
   int blocks_p = 0;              // its grid
@@ -127,7 +131,7 @@ struct dg_gpu_ctx {
     long n_send = 0, n_recv = 0;
   };
   std::vector<Halo> halo;
-  std::vector<int4> face_h;    // face codes of mesh 0 (internal numbering), for the chunk schedule
+  std::vector<int4> face_h;    // face codes of mesh 0 (internal numbering), for the wavefront schedule
   std::vector<int> rec_elem_h; // receiver elements of mesh 0 (internal numbering)
   int num_sms = 148;
   int block = 256;

@@ -1,4 +1,4 @@
-// dg_aux.cuh — layout conversions and diagnostics (fetch, load, energy, watchdog).
+// dg_aux.cuh — layout conversions and diagnostics (fetch, load, halo pack/unpack, energy, watchdog).
 #pragma once
 #include "dg_common.cuh"
 

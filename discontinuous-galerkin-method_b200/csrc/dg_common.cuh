@@ -1,14 +1,18 @@
 // dg_common.cuh — shared definitions of the sm_100a kernels of the DG elastic-wave time loop (P2, Np = 6, Nfp = 3).
 //
 // Data layout in HBM (one mesh):
-//   state   U[plane][g], plane = 6*field + node (fields Vx, Vz, Txx, Tzz, Txz), g = e*S + s
-//           (element e in locality order, shot s innermost); plane stride P = Kp*S.
+//   state   30 planes, plane = 6*field + node (fields Vx, Vz, Txx, Tzz, Txz), element e in
+//           locality order, shot s innermost, in one of two layouts (MeshDev::ES / PS give the
+//           value (e, plane, s) at U[e*ES + plane*PS + s] for both):
+//             plane-major   U[plane][e*S + s], plane stride P = Kp*S (kernel bodies with one
+//                           (element, shot) or two elements per thread: a warp reads a plane as
+//                           a contiguous run);
+//             element-major U[e][plane][S] (the packed two-shot bodies: an element's 30 planes
+//                           at compile-time offsets; a warp of S = 64 shots is one element).
 //   geo     R4[Kp]  rx, sx, rz, sz (inverse Jacobian, as fun_DG.c:1162-1165)
 //   mat     R4[Kp]  1/rho, lambda, mu, lambda + 2 mu (the distinct entries of A/B, fun_DG.c:1076-1086)
 //   face    int4[Kp] three face codes and a flag word (see face_code below)
 //   sponge  R[6][Kp] absorb_fun, read only for elements whose flag says they are in the sponge
-// One thread advances one (element, shot) pair; a warp therefore reads every state plane as a
-// contiguous run of 32 values, and for S >= 32 a neighbour gather is a contiguous run as well.
 //
 // Face code: -1 on the outer boundary (exterior state 0, Edge_flag = 0, fun_DG.c:720-738),
 // else nb << 4 | nb_in_sponge << 3 | nb_face << 1 | flip, where nb is the neighbour element,

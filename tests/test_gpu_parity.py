@@ -269,13 +269,14 @@ def test_two_shot_kernels_against_reference(precision, S):
 @pytest.mark.parametrize("persistent", ["0", "1"])
 @pytest.mark.parametrize("precision", ["fp32", "fp32_kahan"])
 @pytest.mark.parametrize("S,block,margin", [(8, 64, None), (2, 256, 0), (64, 128, 0), (128, 256, None),
-                                            (16, 64, 3), (1, 64, None), (1, 128, 0)])
+                                            (16, 64, 3), (15, 64, None), (1, 64, None), (1, 128, 0)])
 def test_wavefront_step_equals_two_pass_step(precision, S, block, margin, persistent, monkeypatch):
     """One launch per step (k_step_wave / k_step_wave_p, RCM order) gives the same bits as the
     two launches, for warps covering 64 elements (one shot, two elements per thread), many
-    elements (2 shots), one element (64) and half an element (128), with no lag margin (every
-    stress update waits on velocity updates still in flight), one block per ticket and resident
-    blocks looping over the tickets."""
+    elements (2 shots), one element (64) and half an element (128), an odd shot count padded
+    with a silent shot (15 -> 16), with no lag margin (every stress update waits on velocity
+    updates still in flight), one block per ticket and resident blocks looping over the
+    tickets."""
     monkeypatch.setenv("DG_WAVE_PERSISTENT", persistent)
     if margin is not None:
         monkeypatch.setenv("DG_WAVE_MARGIN", str(margin))

@@ -180,6 +180,17 @@ struct dg_gpu_ctx {
     if (!h.empty()) CK(cudaMemcpyAsync(*out, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     return DG_OK;
   }
+  // free one buffer made by alloc/upload (after the stream has finished with it)
+  void release(const void* p) {
+    if (!p) return;
+    for (size_t k = 0; k < allocs.size(); k++)
+      if (allocs[k] == p) {
+        cudaStreamSynchronize(stream);
+        cudaFree(allocs[k]);
+        allocs.erase(allocs.begin() + (long)k);
+        return;
+      }
+  }
 };
 
 namespace {
@@ -649,6 +660,15 @@ int build_wave(dg_gpu_ctx* c) {
     }
     if (rlist.empty()) rlist.push_back(0);
   }
+  // a new schedule for a new block size: the previous one's buffers are no longer needed
+  c->release(c->wv.wait);
+  c->release(c->wv.rec_start);
+  c->release(c->wv.rec_list);
+  c->release(c->wv.vflag);
+  c->release(c->wv.tickets);
+  c->release(c->wv.ptk);
+  c->release(c->wv.error);
+  c->wv = Wave{};
   int *d_wait, *d_rs, *d_rl;
   unsigned* d_flag;
   unsigned long long* d_tk;

@@ -308,11 +308,11 @@ static inline int outside_box(double x, double z, const dgh_setup_in *in)
 /* node number (1-based) of a triangle's corner slot: slot 0 -> 6, 1 -> 1, 2 -> 3 (fun_DG.c:329-340) */
 static const long corner_node[3] = {6, 1, 3};
 
-static const double *g_sort_x; /* positions being sorted by match_vertices (single-threaded use) */
+typedef struct { double x; long q; } x_index; /* a query position's x and its index */
 static int cmp_by_x(const void *a, const void *b)
 {
-	const double xa = g_sort_x[2 * *(const long *)a], xb = g_sort_x[2 * *(const long *)b];
-	return xa < xb ? -1 : (xa > xb ? 1 : (*(const long *)a < *(const long *)b ? -1 : 1));
+	const x_index *u = a, *v = b;
+	return u->x < v->x ? -1 : (u->x > v->x ? 1 : (u->q < v->q ? -1 : (u->q > v->q)));
 }
 static int cmp_long_pair(const void *a, const void *b)
 {
@@ -326,35 +326,31 @@ static int cmp_long_pair(const void *a, const void *b)
 static void match_vertices(const double *Point, long P, const double *pos, long n, double tol, int last, long *out)
 {
 	if (n <= 0) return;
-	long *ord = malloc(sizeof(long) * (size_t)n);
-	double *xs = malloc(sizeof(double) * (size_t)n);
-	for (long q = 0; q < n; q++) { out[q] = -1; if (ord) ord[q] = q; }
-	if (!ord || !xs) { /* out of memory: fall back to the direct scan */
+	x_index *ord = malloc(sizeof(x_index) * (size_t)n);
+	for (long q = 0; q < n; q++) out[q] = -1;
+	if (!ord) { /* out of memory: fall back to the direct scan */
 		for (long q = 0; q < n; q++)
 			for (long i = 0; i < P; i++)
 				if (fabs(Point[i * 2] - pos[q * 2]) < tol && fabs(Point[i * 2 + 1] - pos[q * 2 + 1]) < tol) {
 					out[q] = i + 1;
 					if (!last) break;
 				}
-		free(ord); free(xs);
 		return;
 	}
-	g_sort_x = pos;
-	qsort(ord, (size_t)n, sizeof(long), cmp_by_x);
-	for (long q = 0; q < n; q++) xs[q] = pos[2 * ord[q]];
+	for (long q = 0; q < n; q++) { ord[q].x = pos[2 * q]; ord[q].q = q; }
+	qsort(ord, (size_t)n, sizeof(x_index), cmp_by_x);
 	for (long i = 0; i < P; i++) {
 		const double px = Point[i * 2], pz = Point[i * 2 + 1];
 		/* queries with x > px - tol - a margin (the exact test below decides) */
 		const double lo_x = px - 2 * tol;
 		long lo = 0, hi = n;
-		while (lo < hi) { const long mid = (lo + hi) / 2; if (xs[mid] < lo_x) lo = mid + 1; else hi = mid; }
-		for (long k = lo; k < n && xs[k] <= px + 2 * tol; k++) {
-			const long q = ord[k];
+		while (lo < hi) { const long mid = (lo + hi) / 2; if (ord[mid].x < lo_x) lo = mid + 1; else hi = mid; }
+		for (long k = lo; k < n && ord[k].x <= px + 2 * tol; k++) {
+			const long q = ord[k].q;
 			if (fabs(px - pos[q * 2]) < tol && fabs(pz - pos[q * 2 + 1]) < tol && (last || out[q] < 0)) out[q] = i + 1;
 		}
 	}
 	free(ord);
-	free(xs);
 }
 
 int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)

@@ -8,7 +8,7 @@ neighbours owned by other parts), built from the whole mesh's set-up arrays, and
 a neighbouring part needs travel, point to point:
 
 * `partition` — recursive coordinate bisection of the triangle centroids into balanced parts
-  (any owner array works, e.g. a METIS epart);
+  (any owner array works, e.g. a METIS epart file through `read_epart`);
 * `split` — the part meshes (dicts for `engine.Engine`) and the exchange plan: for every pair
   of parts the owned triangles one sends and the ghosts the other receives, in the same order;
 * `SplitRun` — steps all parts in turn (velocity half, exchange of Vx/Vz, stress half, exchange
@@ -56,6 +56,19 @@ def partition(mesh: dict, parts: int) -> np.ndarray:
         rec(order[cut:], first + left, n - left)
 
     rec(np.arange(len(c)), 0, parts)
+    return owner
+
+
+def read_epart(path: str, K: int | None = None) -> np.ndarray:
+    """Owner array from a METIS element-partition file (one 0-based part number per triangle,
+    one per line, as the reference's MPI driver reads input_files/mesh/*.epart.N with
+    epartinput, DG_leap_Frog_MPI.c:204-207)."""
+    with open(path) as f:
+        owner = np.array([int(t) for t in f.read().split()], dtype=np.int64)
+    if K is not None and owner.size != K:
+        raise ValueError("epart has %d entries for %d triangles" % (owner.size, K))
+    if owner.size and owner.min() < 0:
+        raise ValueError("negative part number in epart")
     return owner
 
 

@@ -143,3 +143,18 @@ def test_halo_transfer_between_gloo_ranks():
         p.join(180)
         assert p.exitcode == 0
     assert all(out[r] for r in range(world))
+
+
+def test_epart_file_round_trip(whole, tmp_path):
+    """A partition written as a METIS epart file reads back as the same owner array, and a split
+    built from it passes the plan checks."""
+    s, mesh = whole
+    owner = dec.partition(mesh, 3)
+    path = str(tmp_path / "model.epart.3")
+    pkg.meshgen.write_epart(path, s.K, owner)
+    back = dec.read_epart(path, s.K)
+    assert np.array_equal(back, owner)
+    parts = dec.split(mesh, back)
+    assert sum(p.own.size for p in parts) == s.K
+    with pytest.raises(ValueError):
+        dec.read_epart(path, s.K + 1)

@@ -353,24 +353,33 @@ def run_ours(args):
 
     # ---- accuracy: the batch against FP64 over the first steps -----------------------------
     def traces(engine):
-        out = []
+        """All traces, and each mesh's slice of them."""
+        out, cuts = [], [0]
         for k, x in enumerate(ws):
             for m in range(x.shots):
                 out += [engine.fetch("trace_x", k, m).ravel(), engine.fetch("trace_z", k, m).ravel()]
-        return np.concatenate(out)
+            cuts.append(sum(a.size for a in out))
+        return np.concatenate(out), cuts
 
     e.reset()
     e.step(acc_steps)
-    tr = traces(e)
+    tr, cuts = traces(e)
     e.close()
     accuracy = None
     if args.precision != "fp64":
         with eng.Engine(meshes, "fp64", device=device) as e64:
             e64.step(acc_steps)
-            tr64 = traces(e64)
+            tr64, _ = traces(e64)
         if np.linalg.norm(tr64) > 0:
             accuracy = {"trace_rel_l2_vs_fp64": float(np.linalg.norm(tr - tr64) / np.linalg.norm(tr64)),
                         "steps": acc_steps, "shots": S_tot}
+            if len(ws) > 1:  # each mesh on its own (None: its traces are still zero)
+                per = []
+                for a, b in zip(cuts[:-1], cuts[1:]):
+                    n64 = np.linalg.norm(tr64[a:b])
+                    per.append(float(np.linalg.norm(tr[a:b] - tr64[a:b]) / n64) if n64 > 0 else None)
+                accuracy["per_mesh"] = per
+                accuracy["per_mesh_max"] = max((v for v in per if v is not None), default=None)
         else:  # the wave has not reached a receiver yet: nothing to compare
             accuracy = {"trace_rel_l2_vs_fp64": None, "steps": acc_steps, "shots": S_tot,
                         "note": "FP64 traces still zero after %d steps (source delay); the long-run "

@@ -116,6 +116,7 @@ struct dg_gpu_ctx {
   // layout); S >= 2 two shots per thread (element-major layout U[e][plane][S])
   int x2 = 0;
   bool mx = false;  // FP32 batch of meshes: per-block dispatch to the packed bodies (k_*_mx)
+  bool x2pm = false; // the two-shot bodies on the plane-major layout (MeshDev::kind 3)
   bool wave = false;  // one launch per step (k_step_wave / k_step_wave_p), RCM order, schedule in wv
   bool wave_persistent = false;  // k_step_wave_p: resident blocks looping over the tickets
   int margin_warps_per_sm = 10;  // lag margin of the wavefront step beyond the unit bandwidth
@@ -576,7 +577,7 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
   for (size_t k = 0; k < md.size(); k++) {
     MeshHostInfo& h = c->mi[k];
     const long long lanes =
-        h.kind == 1 ? h.Kp / 2 : (h.kind == 2 ? (long long)h.K * (h.S_pad / 2) : (long long)h.K * h.S_pad);
+        h.kind == 1 ? h.Kp / 2 : (h.kind >= 2 ? (long long)h.K * (h.S_pad / 2) : (long long)h.K * h.S_pad);
     h.elem_blocks = (int)((lanes + B - 1) / B);
     h.rec_blocks = (h.n_rec * h.S_pad + B - 1) / B;
     md[k].n_elem_blocks = h.elem_blocks;
@@ -720,14 +721,15 @@ int build_wave(dg_gpu_ctx* c) {
   return DG_OK;
 }
 
-// shot counts with a two-shot FP32 kernel instance
+// shot counts with a two-shot FP32 kernel instance (element-major), and with a plane-major one
 bool x2_supported(int S) { return (S >= 2 && S <= 16 && S % 2 == 0) || S == 32 || S == 64 || S == 128; }
+bool x2pm_supported(int S) { return S >= 4 && S <= 16 && S % 2 == 0; }
 
 // Kernel body and stored shot count for a mesh of S shots: FP32 meshes use the packed bodies —
-// two elements per thread for one shot, two shots per thread from three shots on, an odd count
-// padded with one silent shot — unless the caller asks for one (element, shot) per thread
-// (variant 1); two shots take one (element, shot) per thread unless variant 2 or the wavefront
-// step is asked for.
+// two elements per thread for one shot, two shots per thread from three shots on (plane-major
+// layout up to 14 stored shots, element-major above), an odd count padded with one silent shot
+// — unless the caller asks for one (element, shot) per thread (variant 1); two shots take one
+// (element, shot) per thread unless variant 2 or 3 or the wavefront step is asked for.
 void choose_kind(int S, long K, bool fp32, int variant, bool want_wave, int& kind, int& S_pad) {
   kind = 0;
   S_pad = S;
@@ -739,10 +741,15 @@ void choose_kind(int S, long K, bool fp32, int variant, bool want_wave, int& kin
   // two shots: one (element, shot) per thread unless asked otherwise.  The packed body would
   // give each thread a whole element, so a warp's loads scatter over 32 element records
   // (200k elements: 245 G DOF-updates/s against 163 G; from 4 shots on the packed body wins)
-  if (S == 2 && variant != 2 && !want_wave) return;
+  if (S == 2 && variant != 2 && variant != 3 && !want_wave) return;
   const int even = S + (S & 1);
   if (x2_supported(even) && (long long)K * (even / 2) < (1LL << 31)) {
-    kind = 2;
+    // plane-major packed body for 4..14 stored shots: the element-major one scatters a warp's
+    // loads over a few element records (200k elements, two launches: 4 shots 333 G against
+    // 269 G DOF-updates/s, 6: 357 against 284, 8: 382 against 358, 16: equal); the wavefront
+    // step needs the element-major layout
+    const bool pm = x2pm_supported(even) && (variant == 3 || (variant == 0 && !want_wave && even <= 14));
+    kind = pm ? 3 : 2;
     S_pad = even;
   }
 }
@@ -751,7 +758,7 @@ template <bool KAHAN>
 int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid, bool hv = true, bool ht = true) {
   const dim3 bl(c->block), gv(c->blocks_v), gt(c->blocks_t);
   cudaStream_t st = c->stream;
-  switch (c->x2) {
+  switch (c->x2 + (c->x2pm ? 1000 : 0)) {
     case 1:  // one shot: two elements per thread
       if (hv) k_velocity_x2e<KAHAN><<<gv, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
@@ -763,7 +770,15 @@ int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid, bool hv = true, bool ht = true) {
     if (mid) CK(cudaEventRecord(mid, st));                                             \
     if (ht) k_stress_x2<SS, KAHAN><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);   \
     break;
+#define DG_X2PM(SS)                                                                          \
+  case 1000 + SS:                                                                            \
+    if (hv) k_velocity_x2<SS, KAHAN, true><<<gv, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr); \
+    if (mid) CK(cudaEventRecord(mid, st));                                                   \
+    if (ht) k_stress_x2<SS, KAHAN, true><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);   \
+    break;
     DG_X2(2) DG_X2(4) DG_X2(6) DG_X2(8) DG_X2(10) DG_X2(12) DG_X2(14) DG_X2(16) DG_X2(32) DG_X2(64) DG_X2(128)
+    DG_X2PM(4) DG_X2PM(6) DG_X2PM(8) DG_X2PM(10) DG_X2PM(12) DG_X2PM(14) DG_X2PM(16)
+#undef DG_X2PM
 #undef DG_X2
     default:
       return fail(DG_ERR_UNSUPPORTED, "no two-shot kernel for this shot count");
@@ -1126,7 +1141,10 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
     h.S = p.S;
     h.S_pad = p.S_pad;
     h.kind = p.kind;
-    if (!c->multi) c->x2 = p.kind == 1 ? 1 : (p.kind == 2 ? p.S_pad : 0);
+    if (!c->multi) {
+      c->x2 = p.kind == 1 ? 1 : (p.kind >= 2 ? p.S_pad : 0);
+      c->x2pm = p.kind == 3;
+    }
     if (c->wave) {
       c->face_h = p.face;
       c->rec_elem_h = p.rec_elem;
@@ -1625,7 +1643,8 @@ int dg_gpu_stats_get(dg_gpu_ctx* c, dg_gpu_stats* out) {
   c->stats.kernel_family =
       c->precision == DG_FP64_REF
           ? 0
-          : (c->wave ? (c->wave_persistent ? 6 : 5) : (c->mx ? 4 : (c->x2 == 1 ? 3 : (c->x2 ? 2 : 1))));
+          : (c->wave ? (c->wave_persistent ? 6 : 5)
+                     : (c->mx ? 4 : (c->x2 == 1 ? 3 : (c->x2 ? (c->x2pm ? 7 : 2) : 1))));
   c->stats.bytes_per_step = c->wave ? c->bytes_wave : c->bytes_two_pass;
   *out = c->stats;
   return DG_OK;

@@ -2,7 +2,8 @@
 // counts, time steps and step counts.  Each block belongs to one mesh (block table) and runs the
 // kernel body that suits that mesh: two elements per thread for one shot, two shots per thread
 // (packed FP32x2, element-major layout) for even shot counts — odd counts above one are padded
-// on the host with one silent shot — and one (element, shot) per thread otherwise.
+// on the host with one silent shot, on element-major or (kind 3) plane-major state — and one
+// (element, shot) per thread otherwise.
 #pragma once
 #include "dg_common.cuh"
 #include "dg_step_generic.cuh"
@@ -12,6 +13,7 @@ namespace dg {
 
 #define DG_MX_SHOTS(CALL) \
   CALL(2) CALL(4) CALL(6) CALL(8) CALL(10) CALL(12) CALL(14) CALL(16) CALL(32) CALL(64) CALL(128)
+#define DG_MX_PM_SHOTS(CALL) CALL(4) CALL(6) CALL(8) CALL(10) CALL(12) CALL(14) CALL(16)
 
 template <bool KAHAN>
 __global__ void __launch_bounds__(256, 2) k_velocity_mx(const __grid_constant__ Ops<float> ops,
@@ -34,6 +36,17 @@ __global__ void __launch_bounds__(256, 2) k_velocity_mx(const __grid_constant__ 
     break;
       DG_MX_SHOTS(DG_MX_V)
 #undef DG_MX_V
+      default:
+        break;
+    }
+  } else if (m.kind == 3) {
+    switch (m.S) {
+#define DG_MX_VP(SS) \
+  case SS:           \
+    velocity_x2_body<SS, KAHAN, true>(ops2, m, b.y, t); \
+    break;
+      DG_MX_PM_SHOTS(DG_MX_VP)
+#undef DG_MX_VP
       default:
         break;
     }
@@ -67,6 +80,17 @@ __global__ void __launch_bounds__(256, 2) k_stress_mx(const __grid_constant__ Op
     break;
       DG_MX_SHOTS(DG_MX_T)
 #undef DG_MX_T
+      default:
+        break;
+    }
+  } else if (m.kind == 3) {
+    switch (m.S) {
+#define DG_MX_TP(SS) \
+  case SS:           \
+    stress_x2_body<SS, KAHAN, false, true>(ops2, m, b.y, t); \
+    break;
+      DG_MX_PM_SHOTS(DG_MX_TP)
+#undef DG_MX_TP
       default:
         break;
     }

@@ -44,21 +44,25 @@ __device__ __forceinline__ void kahan2(float2& u, float2& c, float2 d) {
 
 // Bodies take the mesh, the block's index within that mesh and the step; the __global__
 // wrappers below (one mesh) and the multi-mesh dispatchers (dg_step_multi.cuh) call them.
-template <int S, bool KAHAN>
+// PM: plane-major layout U[plane][e*S + s] (plane stride Kp*S/2 float2) instead of the
+// element-major U[e][plane][S]; the arithmetic is the same.
+template <int S, bool KAHAN, bool PM = false>
 __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
   constexpr int H = S / 2;    // float2 lanes per element
-  constexpr int ES = 30 * H;  // element stride in float2
+  constexpr int ES = 30 * H;  // element stride in float2 (element-major)
+  const long long EO = PM ? H : ES;                   // element offset
+  const long long PS = PM ? (long long)m.Kp * H : H;  // plane stride
   const int g = lb * blockDim.x + threadIdx.x;
   if (g >= m.K * H) return;
   const int e = g / H, q = g - e * H;
-  float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * ES + q;
+  float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * EO + q;
 
   float2 txx[NP], tzz[NP], txz[NP];
 #pragma unroll
   for (int i = 0; i < NP; i++) {
-    txx[i] = Ue[(12 + i) * H];
-    tzz[i] = Ue[(18 + i) * H];
-    txz[i] = Ue[(24 + i) * H];
+    txx[i] = Ue[(12 + i) * PS];
+    tzz[i] = Ue[(18 + i) * PS];
+    txz[i] = Ue[(24 + i) * PS];
   }
   const int4 fc = __ldg(m.face + e);
   const float4 gm = __ldg(m.geo + e);
@@ -91,13 +95,13 @@ __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<
       for (int k = 0; k < NF; k++) { pxx[k] = f2(0.f); pzz[k] = f2(0.f); pxz[k] = f2(0.f); }
     } else {
       const int nb = code >> 4, nf = (code >> 1) & 3, flip = code & 1;
-      const float2* __restrict__ Un = reinterpret_cast<const float2*>(m.U) + (long long)nb * ES + q;
+      const float2* __restrict__ Un = reinterpret_cast<const float2*>(m.U) + (long long)nb * EO + q;
 #pragma unroll
       for (int k = 0; k < NF; k++) {
         const int node = face_node(nf, flip ? 2 - k : k);
-        pxx[k] = Un[(12 + node) * H];
-        pzz[k] = Un[(18 + node) * H];
-        pxz[k] = Un[(24 + node) * H];
+        pxx[k] = Un[(12 + node) * PS];
+        pzz[k] = Un[(18 + node) * PS];
+        pxz[k] = Un[(24 + node) * PS];
       }
       if (code & 8) {
 #pragma unroll
@@ -153,12 +157,12 @@ __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<
   // V = a V (+ source on Vz) + dt/rho * rhs
   float2 vx[NP], vz[NP], cx[NP], cz[NP];
 #pragma unroll
-  for (int i = 0; i < NP; i++) { vx[i] = Ue[(0 + i) * H]; vz[i] = Ue[(6 + i) * H]; }
+  for (int i = 0; i < NP; i++) { vx[i] = Ue[(0 + i) * PS]; vz[i] = Ue[(6 + i) * PS]; }
   float2* __restrict__ Ce = nullptr;
   if (KAHAN) {
-    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * ES + q;
+    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * EO + q;
 #pragma unroll
-    for (int i = 0; i < NP; i++) { cx[i] = Ce[(0 + i) * H]; cz[i] = Ce[(6 + i) * H]; }
+    for (int i = 0; i < NP; i++) { cx[i] = Ce[(0 + i) * PS]; cz[i] = Ce[(6 + i) * PS]; }
   }
   if (own_sponge) {
 #pragma unroll
@@ -190,23 +194,23 @@ __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<
       vx[i] = fma2(step, hx[i], vx[i]);
       vz[i] = fma2(step, hz[i], add2(vz[i], src[i]));
     }
-    Ue[(0 + i) * H] = vx[i];
-    Ue[(6 + i) * H] = vz[i];
+    Ue[(0 + i) * PS] = vx[i];
+    Ue[(6 + i) * PS] = vz[i];
   }
   if (KAHAN) {
 #pragma unroll
-    for (int i = 0; i < NP; i++) { Ce[(0 + i) * H] = cx[i]; Ce[(6 + i) * H] = cz[i]; }
+    for (int i = 0; i < NP; i++) { Ce[(0 + i) * PS] = cx[i]; Ce[(6 + i) * PS] = cz[i]; }
   }
 }
 
-template <int S, bool KAHAN>
+template <int S, bool KAHAN, bool PM = false>
 __global__ void __launch_bounds__(256, 2) k_velocity_x2(const __grid_constant__ Ops2 ops,
                                                         const __grid_constant__ MeshDev<float> m,
                                                         Counters* __restrict__ ctr) {
   const long long t = ctr->v;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
   if (t >= m.steps) return;
-  velocity_x2_body<S, KAHAN>(ops, m, blockIdx.x, t);
+  velocity_x2_body<S, KAHAN, PM>(ops, m, blockIdx.x, t);
 }
 
 // Load of a velocity value: plain, or through L2 (FRESH) when other blocks of the same launch
@@ -227,16 +231,18 @@ __device__ __forceinline__ StressConst stress_const(const MeshDev<float>& m, int
 }
 
 // Stress update of lane q (shots 2q, 2q+1) of element e with its constants already loaded.
-template <int S, bool KAHAN, bool FRESH>
+template <int S, bool KAHAN, bool FRESH, bool PM = false>
 __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<float>& m, int e, int q,
                                                const StressConst& k) {
   constexpr int H = S / 2;
   constexpr int ES = 30 * H;
-  float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * ES + q;
+  const long long EO = PM ? H : ES;                   // element offset
+  const long long PS = PM ? (long long)m.Kp * H : H;  // plane stride
+  float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * EO + q;
 
   float2 vx[NP], vz[NP];
 #pragma unroll
-  for (int i = 0; i < NP; i++) { vx[i] = ld_v<FRESH>(Ue + (0 + i) * H); vz[i] = ld_v<FRESH>(Ue + (6 + i) * H); }
+  for (int i = 0; i < NP; i++) { vx[i] = ld_v<FRESH>(Ue + (0 + i) * PS); vz[i] = ld_v<FRESH>(Ue + (6 + i) * PS); }
   const int4 fc = k.fc;
   const float4 gm = k.gm;
   const float4 mt = k.mt;
@@ -274,12 +280,12 @@ __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<fl
       for (int k = 0; k < NF; k++) { px[k] = f2(0.f); pz[k] = f2(0.f); }
     } else {
       const int nb = code >> 4, nf = (code >> 1) & 3, flip = code & 1;
-      const float2* __restrict__ Un = reinterpret_cast<const float2*>(m.U) + (long long)nb * ES + q;
+      const float2* __restrict__ Un = reinterpret_cast<const float2*>(m.U) + (long long)nb * EO + q;
 #pragma unroll
       for (int k = 0; k < NF; k++) {
         const int node = face_node(nf, flip ? 2 - k : k);
-        px[k] = ld_v<FRESH>(Un + (0 + node) * H);
-        pz[k] = ld_v<FRESH>(Un + (6 + node) * H);
+        px[k] = ld_v<FRESH>(Un + (0 + node) * PS);
+        pz[k] = ld_v<FRESH>(Un + (6 + node) * PS);
       }
     }
     float2 fa[NF], fb[NF], fw[NF];
@@ -306,15 +312,15 @@ __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<fl
   float2 txx[NP], tzz[NP], txz[NP], cxx[NP], czz[NP], cxz[NP];
 #pragma unroll
   for (int i = 0; i < NP; i++) {
-    txx[i] = Ue[(12 + i) * H];
-    tzz[i] = Ue[(18 + i) * H];
-    txz[i] = Ue[(24 + i) * H];
+    txx[i] = Ue[(12 + i) * PS];
+    tzz[i] = Ue[(18 + i) * PS];
+    txz[i] = Ue[(24 + i) * PS];
   }
   float2* __restrict__ Ce = nullptr;
   if (KAHAN) {
-    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * ES + q;
+    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * EO + q;
 #pragma unroll
-    for (int i = 0; i < NP; i++) { cxx[i] = Ce[(12 + i) * H]; czz[i] = Ce[(18 + i) * H]; cxz[i] = Ce[(24 + i) * H]; }
+    for (int i = 0; i < NP; i++) { cxx[i] = Ce[(12 + i) * PS]; czz[i] = Ce[(18 + i) * PS]; cxz[i] = Ce[(24 + i) * PS]; }
   }
   if (fc.w & 1) {
 #pragma unroll
@@ -339,28 +345,28 @@ __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<fl
       tzz[i] = add2(tzz[i], dzz);
       txz[i] = add2(txz[i], dxz);
     }
-    Ue[(12 + i) * H] = txx[i];
-    Ue[(18 + i) * H] = tzz[i];
-    Ue[(24 + i) * H] = txz[i];
+    Ue[(12 + i) * PS] = txx[i];
+    Ue[(18 + i) * PS] = tzz[i];
+    Ue[(24 + i) * PS] = txz[i];
   }
   if (KAHAN) {
 #pragma unroll
     for (int i = 0; i < NP; i++) {
-      Ce[(12 + i) * H] = cxx[i]; Ce[(18 + i) * H] = czz[i]; Ce[(24 + i) * H] = cxz[i];
+      Ce[(12 + i) * PS] = cxx[i]; Ce[(18 + i) * PS] = czz[i]; Ce[(24 + i) * PS] = cxz[i];
     }
   }
 }
 
-template <int S, bool KAHAN, bool FRESH = false>
+template <int S, bool KAHAN, bool FRESH = false, bool PM = false>
 __device__ __forceinline__ void stress_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
   constexpr int H = S / 2;
   const int g = lb * blockDim.x + threadIdx.x;
   if (g >= m.K * H) return;
   const int e = g / H, q = g - e * H;
-  stress_x2_core<S, KAHAN, FRESH>(ops, m, e, q, stress_const(m, e));
+  stress_x2_core<S, KAHAN, FRESH, PM>(ops, m, e, q, stress_const(m, e));
 }
 
-template <int S, bool KAHAN>
+template <int S, bool KAHAN, bool PM = false>
 __global__ void __launch_bounds__(256, 2) k_stress_x2(const __grid_constant__ Ops2 ops,
                                                       const __grid_constant__ MeshDev<float> m,
                                                       Counters* __restrict__ ctr) {
@@ -368,7 +374,7 @@ __global__ void __launch_bounds__(256, 2) k_stress_x2(const __grid_constant__ Op
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
   if (t >= m.steps) return;
   if ((int)blockIdx.x >= m.n_elem_blocks) { record(m, blockIdx.x - m.n_elem_blocks, t); return; }
-  stress_x2_body<S, KAHAN>(ops, m, blockIdx.x, t);
+  stress_x2_body<S, KAHAN, false, PM>(ops, m, blockIdx.x, t);
 }
 
 // -------------------------------------------------------------------------------------------

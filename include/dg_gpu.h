@@ -97,7 +97,8 @@ typedef struct {
 	int watchdog_every;  /* check the velocity fields for NaN/Inf every k steps (0: off) */
 	const char *tune_cache; /* file that keeps autotune results between runs (NULL: none) */
 	int variant;         /* FP32 kernels: 0 automatic, 1 one (element, shot) per thread,
-	                        2 packed FP32x2 kernels (two elements or two shots per thread) */
+	                        2 packed FP32x2 kernels (two elements or two shots per thread; element-major
+	                        state for two shots per thread), 3 the same with plane-major state for 4-16 shots */
 	int wavefront;       /* one launch per step that keeps the state in flight in L2 (single FP32 mesh
 	                        of 1, 2, 4, ..., 128 shots): 0 automatic (on from 16 shots), 1 on, -1 off */
 } dg_gpu_opts;
@@ -115,7 +116,8 @@ typedef struct {
 	                          2 two shots per thread (packed FP32x2), 3 two elements per thread (packed),
 	                          4 FP32 batch of meshes, each block running its mesh's packed body,
 	                          5 wavefront step (one launch per step, two shots per thread, one block per ticket),
-	                          6 the same with resident blocks that loop over the tickets (FP32 default) */
+	                          6 the same with resident blocks that loop over the tickets (FP32 default),
+	                          7 two shots per thread on plane-major state (FP32, 3-14 shots) */
 } dg_gpu_stats;
 
 void dg_gpu_default_opts(dg_gpu_opts *opts);

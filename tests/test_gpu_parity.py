@@ -367,6 +367,22 @@ def test_autotuned_schedule_gives_the_same_bits_and_is_cached(precision, S, tmp_
     assert stats[1]["kernel_family"] == stats[2]["kernel_family"]
 
 
+@pytest.mark.parametrize("precision,S", [("fp32", 4), ("fp32", 6), ("fp32_kahan", 5), ("fp32", 16)])
+def test_plane_major_and_element_major_packed_kernels_give_the_same_bits(precision, S):
+    """The packed two-shot bodies on plane-major state (family 7) and on element-major state
+    (family 2) do the same arithmetic: fields and traces agree bit for bit."""
+    g = Golden("slope_coupled")
+    m, _ = _repeat_shots(g.setup_arrays(), S, pattern=(0,))
+    out = []
+    for variant, fam in ((2, 2), (3, 7)):
+        with eng.Engine(m, precision, variant=variant, wavefront=-1) as e:
+            assert e.stats()["kernel_family"] == fam
+            e.step(g.steps)
+            out.append([e.fetch(f, 0, s) for s in (0, S - 1) for f in FIELDS] + [e.fetch("trace_z", 0, S - 1)])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
 def test_two_shot_and_one_shot_kernels_agree():
     g = Golden("slope_coupled")
     m, _ = _repeat_shots(g.setup_arrays(), 4, pattern=(0,))

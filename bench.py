@@ -128,17 +128,25 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(args):
+def dist_setup(args, join: bool = True):
+    """Rank, world size and local rank from the launcher's environment; with `join` and more than
+    one rank, also the process group.  Under NCCL each rank binds its own GPU (LOCAL_RANK) before
+    the group exists, so that NCCL's communicator and the barrier's synchronize both use it."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
-    if world > 1:
+    if world > 1 and join:
         import datetime
 
+        import torch
         import torch.distributed as dist
         backend = os.environ.get("DG_BENCH_BACKEND", "nccl")
-        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+        kw = {}
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            kw["device_id"] = torch.device("cuda", local)
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120), **kw)
     return rank, world, local, dist
 
 
@@ -210,7 +218,8 @@ def cpu_reference(w, steps_hint: float = 12.0):
 
 
 def run_reference_arm(args):
-    rank, world, local, dist = dist_setup(args)
+    # rank 0 alone times the CPU code; no collective, so no process group is joined
+    rank, world, local, dist = dist_setup(args, join=False)
     if rank != 0:
         return 0
     ctor, desc = WORKLOADS[args.workload]

@@ -24,14 +24,12 @@ def _free_port():
 
 
 def _worker(rank, world, port, out):
-    import datetime
-
-    import torch.distributed as dist
     sys.path.insert(0, ROOT)
     import bench
     os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
-                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank), "DG_BENCH_BACKEND": "gloo"})
+    r, wsz, local, dist = bench.dist_setup(None)
+    assert (r, wsz, local) == (rank, world, rank) and dist.get_backend() == "gloo"
     local_ms = 10.0 * (rank + 1)
     value, t_max = bench.weak_scaling_value(1000.0, 5, local_ms, world, dist, "cpu")
     w = bench.WORKLOADS["multishot"][0](10, rank)
@@ -62,8 +60,11 @@ def test_two_ranks_weak_scaling_and_distinct_shots():
 def test_reference_arm_is_rank0_only(monkeypatch):
     sys.path.insert(0, ROOT)
     import bench
-    monkeypatch.setenv("WORLD_SIZE", "1")
+    monkeypatch.setenv("WORLD_SIZE", "2")
     monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("LOCAL_RANK", "1")
     args = bench.argparse.Namespace(gpus=2, steps=1, warmup=3, impl="reference", workload="square",
                                     no_cpu_baseline=False)
     assert bench.run_reference_arm(args) == 0     # returns before any work on a non-zero rank
+    import torch.distributed as dist
+    assert not dist.is_initialized()              # and joins no process group

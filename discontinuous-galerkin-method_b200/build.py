@@ -1,9 +1,9 @@
 """In-tree build of the native libraries (no JIT cache: the built .so files sit next to this file).
 
 * ``libdg_host.so`` — host set-up (csrc/dg_host.c), gcc, ``-O2 -ffp-contract=off`` so its
-  arrays equal the reference host code's.
+  arrays equal the reference host code's; ``-fopenmp`` for its per-element loops.
 * ``libdg_gpu.so``  — the sm_100a engine and its C ABI (csrc/dg_gpu.cu), nvcc
-  ``-gencode arch=compute_100a,code=sm_100a``.
+  ``-gencode arch=compute_100a,code=sm_100a``; the host side of ``dg_gpu_init`` uses OpenMP.
 """
 from __future__ import annotations
 
@@ -25,7 +25,7 @@ GPU_DEPS = GPU_SRC + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endsw
     [os.path.join(INCLUDE, "dg_gpu.h")]
 
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-              "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr", "-Xptxas", "-v"]
+              "-Xcompiler", "-fPIC,-fopenmp", "-shared", "--expt-relaxed-constexpr", "-Xptxas", "-v", "-lgomp"]
 
 
 def _stale(target, deps):
@@ -44,7 +44,7 @@ def host_library(force: bool = False) -> str:
     deps = HOST_SRC + [os.path.join(INCLUDE, "dg_host.h")]
     if force or _stale(HOST_SO, deps):
         tmp = HOST_SO + ".tmp%d" % os.getpid()
-        subprocess.run([_cc(), "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-Wall",
+        subprocess.run([_cc(), "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-Wall",
                         "-I" + INCLUDE, "-o", tmp] + HOST_SRC + ["-lm"], check=True)
         os.replace(tmp, HOST_SO)
     return HOST_SO

@@ -18,6 +18,9 @@
 #include "dg_step_wave.cuh"
 #include "dg_step_x2.cuh"
 
+#include <omp.h>
+#include <parallel/algorithm>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -228,8 +231,21 @@ std::vector<int> rcm_order(const dg_gpu_mesh& m, long K) {
     return (n >= 0 && n < K && n != e) ? n : -1;
   };
   std::vector<int> deg(K, 0);
+#pragma omp parallel for schedule(static)
   for (long e = 0; e < K; e++)
     for (int f = 0; f < 3; f++) deg[e] += nbr(e, f) >= 0;
+  // every element's neighbours in visiting order (increasing degree, then number), -1 padded
+  std::vector<int> nbt((size_t)K * 3);
+#pragma omp parallel for schedule(static)
+  for (long e = 0; e < K; e++) {
+    int out[3] = {-1, -1, -1}, n = 0;
+    for (int f = 0; f < 3; f++) {
+      const long x = nbr(e, f);
+      if (x >= 0) out[n++] = (int)x;
+    }
+    std::sort(out, out + n, [&](int a, int b) { return deg[a] < deg[b] || (deg[a] == deg[b] && a < b); });
+    for (int q = 0; q < 3; q++) nbt[e * 3 + q] = out[q];
+  }
   std::vector<int> stamp(K, -1), queue(K);
   std::vector<char> placed(K, 0);
   std::vector<int> seq;
@@ -237,11 +253,7 @@ std::vector<int> rcm_order(const dg_gpu_mesh& m, long K) {
   int pass = 0;
   auto sorted_nbrs = [&](long e, long out[3]) {
     int n = 0;
-    for (int f = 0; f < 3; f++) {
-      const long x = nbr(e, f);
-      if (x >= 0) out[n++] = x;
-    }
-    std::sort(out, out + n, [&](long a, long b) { return deg[a] < deg[b] || (deg[a] == deg[b] && a < b); });
+    for (int q = 0; q < 3 && nbt[e * 3 + q] >= 0; q++) out[n++] = nbt[e * 3 + q];
     return n;
   };
   for (long s0 = 0; s0 < K; s0++) {
@@ -313,9 +325,13 @@ int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
   p.Kp = (int)((K + 31) / 32 * 32);
   const int Kp = p.Kp;
 
+  // The per-element loops below run on OpenMP threads.  A loop that finds invalid input records
+  // the first offending element (in loop order) and, after the loop, that element is checked
+  // again to report the error a sequential loop would have stopped at.
+
   // geometry per caller element, as Dx_Dz (fun_DG.c:1150-1165)
   std::vector<double> cx(K), cz(K), rxa(K * 4);
-  for (long e = 0; e < K; e++) {
+  auto geometry = [&](long e) -> int {
     double X[3], Z[3];
     for (int v = 0; v < 3; v++) {
       long pt = m.Triangle[e * 3 + v] - 1;
@@ -334,7 +350,13 @@ int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
     rxa[e * 4 + 3] = Xr / J;
     cx[e] = (X[0] + X[1] + X[2]) / 3.0;
     cz[e] = (Z[0] + Z[1] + Z[2]) / 3.0;
-  }
+    return DG_OK;
+  };
+  long bad = K;
+#pragma omp parallel for schedule(static) reduction(min : bad)
+  for (long e = 0; e < K; e++)
+    if (geometry(e) != DG_OK) bad = std::min(bad, e);
+  if (bad < K) return geometry(bad);
 
   // locality order: Hilbert curve of centroids (1), or reverse Cuthill-McKee (2) for the
   // wavefront step, which needs every element's neighbours close to it in the numbering
@@ -349,20 +371,25 @@ int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
       z0 = std::min(z0, cz[e]); z1 = std::max(z1, cz[e]);
     }
     const double span = std::max(x1 - x0, z1 - z0) + 1e-300;
-    std::vector<std::pair<uint64_t, int>> key(K);
+    // (Hilbert index < 2^32) << 32 | element: distinct keys, so any sort gives the same order
+    std::vector<uint64_t> key(K);
+#pragma omp parallel for schedule(static)
     for (long e = 0; e < K; e++) {
       uint32_t ix = (uint32_t)std::min(65535.0, std::floor((cx[e] - x0) / span * 65535.0));
       uint32_t iz = (uint32_t)std::min(65535.0, std::floor((cz[e] - z0) / span * 65535.0));
-      key[e] = {hilbert(ix, iz), (int)e};
+      key[e] = hilbert(ix, iz) << 32 | (uint64_t)e;
     }
-    std::sort(key.begin(), key.end());
-    for (long e = 0; e < K; e++) p.order[e] = key[e].second;
+    __gnu_parallel::sort(key.begin(), key.end());
+#pragma omp parallel for schedule(static)
+    for (long e = 0; e < K; e++) p.order[e] = (int)(key[e] & 0xffffffffu);
   }
   p.new_of_old.assign(K, 0);
+#pragma omp parallel for schedule(static)
   for (long n = 0; n < K; n++) p.new_of_old[p.order[n]] = (int)n;
 
   // sponge flags
   std::vector<char> in_sponge(K, 0);
+#pragma omp parallel for schedule(static)
   for (long e = 0; e < K; e++)
     for (int i = 0; i < 6; i++)
       if (m.absorb_fun[e * 6 + i] != 1.0) in_sponge[e] = 1;
@@ -371,7 +398,7 @@ int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
   p.mat.assign((size_t)Kp * 4, 0.0);
   p.face.assign(Kp, make_int4(-1, -1, -1, 0));
   p.sponge.assign((size_t)6 * Kp, 1.0);
-  for (long n = 0; n < K; n++) {
+  auto element = [&](long n) -> int {
     const long e = p.order[n];
     for (int c = 0; c < 4; c++) p.geo[n * 4 + c] = rxa[e * 4 + c];
     const double* A = m.A + e * 5;
@@ -407,11 +434,19 @@ int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
       codes[f] = (p.new_of_old[nb] << 4) | (in_sponge[nb] ? 8 : 0) | ((found >> 1) << 1) | (found & 1);
     }
     p.face[n] = make_int4(codes[0], codes[1], codes[2], in_sponge[e] ? 1 : 0);
-    if (in_sponge[e]) {
-      p.sponge_elems++;
+    if (in_sponge[e])
       for (int i = 0; i < 6; i++) p.sponge[(size_t)i * Kp + n] = m.absorb_fun[e * 6 + i];
-    }
+    return DG_OK;
+  };
+  bad = K;
+  long sponge_elems = 0;
+#pragma omp parallel for schedule(static) reduction(min : bad) reduction(+ : sponge_elems)
+  for (long n = 0; n < K; n++) {
+    if (element(n) != DG_OK) bad = std::min(bad, n);
+    sponge_elems += in_sponge[p.order[n]];
   }
+  if (bad < K) return element(bad);
+  p.sponge_elems = sponge_elems;
   // padded (silent) shots: no source element, zero source vector
   p.src_elem.assign(p.S_pad, -1);
   p.src_fun.assign((size_t)p.S_pad * 6, 0.0);
@@ -434,6 +469,7 @@ int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
     p.Dz.assign((size_t)36 * Kp, 0.0);
     p.Q.assign((size_t)30 * Kp, 0.0);
     p.AB.assign((size_t)10 * Kp, 0.0);
+#pragma omp parallel for schedule(static)
     for (long n = 0; n < K; n++) {
       const long e = p.order[n];
       for (int q = 0; q < 36; q++) {
@@ -480,6 +516,7 @@ int upload_mesh(dg_gpu_ctx* c, const dg_gpu_mesh& m, Prepared& p, MeshDev<R>& d)
     CK(cudaMemsetAsync(d.C, 0, sizeof(R) * NPLANES * d.P, c->stream));
   }
   std::vector<R4> geo(p.Kp), mat(p.Kp);
+#pragma omp parallel for schedule(static)
   for (int n = 0; n < p.Kp; n++) {
     geo[n] = {(R)p.geo[n * 4 + 0], (R)p.geo[n * 4 + 1], (R)p.geo[n * 4 + 2], (R)p.geo[n * 4 + 3]};
     mat[n] = {(R)p.mat[n * 4 + 0], (R)p.mat[n * 4 + 1], (R)p.mat[n * 4 + 2], (R)p.mat[n * 4 + 3]};

@@ -4,6 +4,10 @@
  * Floating-point expressions keep the reference's evaluation order and its libm calls
  * (pow, sqrt, acos, cos, exp) so that, compiled with -ffp-contract=off, every array equals
  * what fun_DG.c produces.  Comments give the reference lines each block follows.
+ *
+ * Per-element loops run on OpenMP threads: each element's values depend on that element alone,
+ * and the reductions over elements (the smallest inscribed radius, counts) are evaluated in
+ * element order after the parallel loop, so the arrays do not depend on the thread count.
  */
 #include "dg_host.h"
 
@@ -69,8 +73,9 @@ static long parse_int_e7(const char *s, long i)
 
 void dgh_quantize_e7(double *x, long n)
 {
-	char buf[64];
+#pragma omp parallel for schedule(static)
 	for (long q = 0; q < n; q++) {
+		char buf[64];
 		int len = snprintf(buf + 8, sizeof buf - 8, "%16.7e", x[q]);
 		memset(buf, ' ', 8);
 		char *e = strchr(buf + 8, 'e');
@@ -339,6 +344,8 @@ static void match_vertices(const double *Point, long P, const double *pos, long 
 	}
 	for (long q = 0; q < n; q++) { ord[q].x = pos[2 * q]; ord[q].q = q; }
 	qsort(ord, (size_t)n, sizeof(x_index), cmp_by_x);
+	/* vertices in parallel; a match keeps the smallest (first) or largest (last) vertex index */
+#pragma omp parallel for schedule(static)
 	for (long i = 0; i < P; i++) {
 		const double px = Point[i * 2], pz = Point[i * 2 + 1];
 		/* queries with x > px - tol - a margin (the exact test below decides) */
@@ -347,7 +354,10 @@ static void match_vertices(const double *Point, long P, const double *pos, long 
 		while (lo < hi) { const long mid = (lo + hi) / 2; if (ord[mid].x < lo_x) lo = mid + 1; else hi = mid; }
 		for (long k = lo; k < n && ord[k].x <= px + 2 * tol; k++) {
 			const long q = ord[k].q;
-			if (fabs(px - pos[q * 2]) < tol && fabs(pz - pos[q * 2 + 1]) < tol && (last || out[q] < 0)) out[q] = i + 1;
+			if (fabs(px - pos[q * 2]) < tol && fabs(pz - pos[q * 2 + 1]) < tol) {
+#pragma omp critical(dgh_match)
+				if (out[q] < 0 || (last ? i + 1 > out[q] : i + 1 < out[q])) out[q] = i + 1;
+			}
 		}
 	}
 	free(ord);
@@ -360,20 +370,27 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 		!in->S3 || !in->Fekete || in->n_shots < 0 || in->n_rec < 0 || in->bound_x <= 0 || in->bound_z <= 0)
 		return DGH_ERR_ARG;
 	const long K = in->K, P = in->n_points;
+	int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
 	for (long e = 0; e < K; e++) {
 		const long *t = in->Triangle + e * 3;
 		for (int v = 0; v < 3; v++)
-			if (t[v] < 1 || t[v] > P) return DGH_ERR_MESH;
-		if (t[0] == t[1] || t[1] == t[2] || t[0] == t[2]) return DGH_ERR_MESH;
+			bad |= t[v] < 1 || t[v] > P;
+		bad |= t[0] == t[1] || t[1] == t[2] || t[0] == t[2];
 		for (int v = 0; v < 3; v++)
-			if (in->neighbor[e * 3 + v] != -1 && (in->neighbor[e * 3 + v] < 1 || in->neighbor[e * 3 + v] > K))
-				return DGH_ERR_MESH;
+			bad |= in->neighbor[e * 3 + v] != -1 && (in->neighbor[e * 3 + v] < 1 || in->neighbor[e * 3 + v] > K);
 	}
+	if (bad) return DGH_ERR_MESH;
 
 	/* Jacobian (fun_DG.c:421-453) and Normals */
 	double *Jac = out->Jacobi ? out->Jacobi : malloc(sizeof(double) * K);
-	if (!Jac) return DGH_ERR_NOMEM;
-	double min_r = 0.0;
+	double *rin = malloc(sizeof(double) * K); /* inscribed diameter per element */
+	if (!Jac || !rin) {
+		if (!out->Jacobi) free(Jac);
+		free(rin);
+		return DGH_ERR_NOMEM;
+	}
+#pragma omp parallel for schedule(static)
 	for (long e = 0; e < K; e++) {
 		tri_xy t = corners(in, e);
 		double L[3];
@@ -415,12 +432,18 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 		double a = L[0], b = L[1], c = L[2];
 		double s = 0.5 * (a + b + c);
 		double S = sqrt(s * (s - a) * (s - b) * (s - c));
-		double r = 2 * S / s;
-		if (e == 0 || r < min_r) min_r = r;
+		rin[e] = 2 * S / s;
 	}
+	double min_r = 0.0;
+	for (long e = 0; e < K; e++)
+		if (e == 0 || rin[e] < min_r) min_r = rin[e];
+	free(rin);
 
 	/* Elastic_A_B (fun_DG.c:1071-1088) with the material formulas of DG_leap_Frog_OpenMP.c:252-253 */
 	double vmax = in->vp[0];
+	for (long e = 1; e < K; e++)
+		if (in->vp[e] > vmax) vmax = in->vp[e];
+#pragma omp parallel for schedule(static)
 	for (long e = 0; e < K; e++) {
 		double Cp = in->vp[e], Cs = in->vs[e], den = in->rho[e];
 		double miu = den * Cs * Cs, lambda = den * Cp * Cp - 2 * miu;
@@ -432,7 +455,6 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 			double *B = out->B + e * 5;
 			B[0] = 1 / den; B[1] = 1 / den; B[2] = lambda; B[3] = lambda + 2 * miu; B[4] = miu;
 		}
-		if (e > 0 && in->vp[e] > vmax) vmax = in->vp[e];
 		if (out->Vp_used) out->Vp_used[e] = in->vp[e];
 	}
 
@@ -467,6 +489,9 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 		for (long q = 0; q < S + R; q++)
 			if (src_node[q] > 0) { pairs[2 * nq] = src_node[q]; pairs[2 * nq + 1] = q; nq++; }
 		qsort(pairs, (size_t)nq, 2 * sizeof(long), cmp_long_pair);
+		/* triangles in parallel; a source keeps the smallest (first) triangle holding its vertex,
+		 * a receiver the largest (last) */
+#pragma omp parallel for schedule(static)
 		for (long e = 0; e < K; e++)
 			for (int v = 0; v < 3; v++) {
 				const long node = in->Triangle[e * 3 + v];
@@ -475,7 +500,8 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 				for (long k = lo; k < nq && pairs[2 * k] == node; k++) {
 					const long q = pairs[2 * k + 1];
 					long *slot = q < S ? src_tri + 2 * q : rec_tri + 2 * (q - S);
-					if (q >= S || slot[0] < 0) { slot[0] = e + 1; slot[1] = corner_node[v]; }  /* sources: first */
+#pragma omp critical(dgh_match)
+					if (slot[0] < 0 || (q < S ? e + 1 < slot[0] : e + 1 > slot[0])) { slot[0] = e + 1; slot[1] = corner_node[v]; }
 				}
 			}
 		free(pairs);
@@ -508,6 +534,7 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 	 * (fun_DG.c:202-281, 879-1006) */
 	{
 		long count = 0, filled = 0;
+#pragma omp parallel for schedule(static) reduction(+ : count, filled)
 		for (long e = 0; e < K; e++) {
 			tri_xy t = corners(in, e);
 			int any = 0;
@@ -548,6 +575,7 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 	if (out->Neighbor || out->Edge || out->Edge_flag || out->Node_Neighbor) {
 		static const int own_a[3] = {0, 1, 2}, own_b[3] = {1, 2, 0};
 		static const int first_of_edge[3] = {0, 1, 0};
+#pragma omp parallel for schedule(static)
 		for (long e = 0; e < K; e++) {
 			const long *T = in->Triangle + e * 3;
 			for (int f = 0; f < 3; f++) {
@@ -583,6 +611,7 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out)
 
 	/* Dx_Dz (fun_DG.c:1137-1192) */
 	if (out->Dx || out->Dz) {
+#pragma omp parallel for schedule(static)
 		for (long e = 0; e < K; e++) {
 			tri_xy t = corners(in, e);
 			double Xr = (t.x[1] - t.x[0]) * 0.5, Zr = (t.z[1] - t.z[0]) * 0.5;

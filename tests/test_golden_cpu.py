@@ -137,3 +137,36 @@ def test_source_and_receiver_vertex_rules_with_duplicate_vertices():
     with pytest.raises(host.HostError) as ei:
         host.build_setup(w, full=False, mesh_arrays=with_duplicate([w.src[0][0] + 5e-4, w.src[0][1]]))
     assert "(-4)" in str(ei.value)
+
+
+_DIGEST = r"""
+import hashlib, importlib, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+P = importlib.import_module("discontinuous-galerkin-method_b200")
+w = P.workloads.random_medium(n_cells_x=100, n_cells_z=50, n_rec=101, corr_len=400.0, steps=20)
+s = P.host.build_setup(w, full=True, n_steps=20)
+h = hashlib.sha1()
+for k in sorted(s.arrays):
+    a = s.arrays[k]
+    if isinstance(a, np.ndarray):
+        h.update(k.encode()); h.update(np.ascontiguousarray(a).tobytes())
+h.update(repr(s.dt).encode())
+print(h.hexdigest())
+"""
+
+
+def test_host_setup_independent_of_thread_count():
+    """The set-up's per-element loops run on OpenMP threads; every array (and dt) is the same
+    with one thread as with several."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = []
+    for n in ("1", "5"):
+        env = dict(os.environ, OMP_NUM_THREADS=n)
+        r = subprocess.run([sys.executable, "-c", _DIGEST, root], env=env, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out.append(r.stdout.strip())
+    assert out[0] == out[1] and len(out[0]) == 40

@@ -82,6 +82,9 @@ template <class R> struct MeshDev {
   long long steps;        // this mesh's wavelet length
   int K, Kp, S, n_rec;
   int n_elem_blocks;      // element blocks of this mesh (grid = these + recorder blocks)
+  int block0;             // one-mesh launches: first element block of the launch, which covers
+                          // blocks [block0, n_elem_blocks) and then the recorder blocks (a window
+                          // of a split mesh's half step; 0 otherwise)
   int kind;               // FP32 kernel body: 0 one (element, shot) per thread, plane-major;
                           // 1 two elements per thread (S = 1); 2 two shots per thread, element-major
   int sponge_elems;
@@ -124,7 +127,7 @@ struct BlockMap { int mesh; int local; };
 template <bool MULTI, class R>
 __device__ __forceinline__ const MeshDev<R>* pick_mesh(const MeshDev<R>& one, const MeshDev<R>* tab,
                                                         const int2* btab, int& local) {
-  if (!MULTI) { local = blockIdx.x; return &one; }
+  if (!MULTI) { local = blockIdx.x + one.block0; return &one; }
   const int2 b = __ldg(btab + blockIdx.x);
   local = b.y;
   return tab + b.x;

@@ -134,6 +134,12 @@ struct dg_gpu_ctx {
     int* d_recv = nullptr;
     long n_send = 0, n_recv = 0;
   };
+  // a half step run in two parts (dg_gpu_half_step_part): the parts of the open half that have
+  // run (bit 0 boundary, bit 1 interior; 0 = none open) and that half.  Mesh 0's elements up to
+  // part_eB (internal numbering) hold every element with a ghost face neighbour, those up to
+  // part_eO every element that is not a ghost (from the halo lists).
+  int part_done = 0, part_half = 0;
+  long part_eB = 0, part_eO = 0;
   std::vector<Halo> halo;
   std::vector<int4> face_h;    // face codes of mesh 0 (internal numbering), for the wavefront schedule
   std::vector<int> rec_elem_h; // receiver elements of mesh 0 (internal numbering)
@@ -1305,7 +1311,8 @@ static int enqueue_steps(dg_gpu_ctx* c, long n, bool timed) {
 
 static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
   if (!c || n < 0) return fail(DG_ERR_ARG, "bad arguments");
-  if (c->half_pending) return fail(DG_ERR_STATE, "a velocity half step is waiting for its stress half");
+  if (c->half_pending || c->part_done)
+    return fail(DG_ERR_STATE, "a half step is waiting for its other half or part");
   if (c->t + n > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
   CK(cudaSetDevice(c->device));
   int rc = enqueue_steps(c, n, timed);
@@ -1548,12 +1555,14 @@ int dg_gpu_reset(dg_gpu_ctx* c) {
   if (!c) return fail(DG_ERR_ARG, "null context");
   CK(cudaSetDevice(c->device));
   c->half_pending = false;
+  c->part_done = 0;
   return zero_state(c);
 }
 
 int dg_gpu_half_step(dg_gpu_ctx* c, int half) {
   if (!c || (half != 0 && half != 1)) return fail(DG_ERR_ARG, "bad arguments");
   if (c->wave) return fail(DG_ERR_UNSUPPORTED, "half steps need the two-launch step (wavefront = -1)");
+  if (c->part_done) return fail(DG_ERR_STATE, "the other part of the open half step has not run");
   if ((half == 0) == c->half_pending)
     return fail(DG_ERR_STATE, half == 0 ? "velocity half again before the stress half" : "stress half without the velocity half");
   if (half == 0 && c->t + 1 > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
@@ -1564,6 +1573,75 @@ int dg_gpu_half_step(dg_gpu_ctx* c, int half) {
   if (half == 1) {
     c->t += 1;
     c->stats.steps_done = c->t;
+  }
+  return DG_OK;
+}
+
+// One part of a half step of mesh 0: the element blocks [0, bB) (boundary) or [bB, bO)
+// (interior), bB and bO the first blocks past the lanes of elements part_eB and part_eO.  A
+// block holds consecutive lanes of consecutive elements in every one-mesh kernel (lane g of
+// element g / lanes-per-element), so each lane of a non-ghost element runs in exactly one part,
+// and every element with a ghost neighbour in the boundary part.  The stress part that closes
+// the half also runs the recorder blocks.  An empty window launches one block past the element
+// blocks (its lanes are out of range and return), so the step counters still advance.
+extern "C++" {
+template <class R> static void set_window(MeshDev<R>& m, int b0, int b1) {
+  m.block0 = b0;
+  m.n_elem_blocks = b1;
+}
+static int launch_part(dg_gpu_ctx* c, int half, int part, bool record) {
+  const MeshHostInfo& h = c->mi[0];
+  const int B = c->block;
+  auto blocks = [&](long n) -> int {
+    const long long lanes = h.kind == 1 ? (n + 1) / 2 : (h.kind >= 2 ? n * (long long)(h.S_pad / 2) : n * (long long)h.S_pad);
+    return (int)std::min<long long>(h.elem_blocks, (lanes + B - 1) / B);
+  };
+  const int bB = blocks(c->part_eB), bO = std::max(bB, blocks(c->part_eO));
+  int b0 = part == 1 ? 0 : bB, b1 = part == 1 ? bB : bO;
+  if (b1 == b0) {
+    b0 = h.elem_blocks;
+    b1 = h.elem_blocks + 1;
+  }
+  const int save_v = c->blocks_v, save_t = c->blocks_t;
+  c->blocks_v = b1 - b0;
+  c->blocks_t = b1 - b0 + (record ? h.rec_blocks : 0);
+  if (c->is_double) set_window(c->md_d[0], b0, b1); else set_window(c->md_f[0], b0, b1);
+  const int rc = launch_step(c, nullptr, nullptr, nullptr, half == 0 ? 1 : 2);
+  c->blocks_v = save_v;
+  c->blocks_t = save_t;
+  if (c->is_double) set_window(c->md_d[0], 0, h.elem_blocks); else set_window(c->md_f[0], 0, h.elem_blocks);
+  return rc;
+}
+}  // extern "C++"
+
+int dg_gpu_half_step_part(dg_gpu_ctx* c, int half, int part) {
+  if (!c || (half != 0 && half != 1) || part < DG_PART_ALL || part > DG_PART_INTERIOR)
+    return fail(DG_ERR_ARG, "bad arguments");
+  if (part == DG_PART_ALL) return dg_gpu_half_step(c, half);
+  if (c->wave) return fail(DG_ERR_UNSUPPORTED, "half steps need the two-launch step (wavefront = -1)");
+  if (c->multi) return fail(DG_ERR_UNSUPPORTED, "half-step parts need a context of one mesh");
+  if (c->halo.empty()) return fail(DG_ERR_STATE, "no halo lists: the parts are defined by the ghosts");
+  if (c->part_done) {
+    if (half != c->part_half) return fail(DG_ERR_STATE, "the other part of the open half step has not run");
+    if (c->part_done & part) return fail(DG_ERR_STATE, "this part of the half step has already run");
+  } else {
+    if ((half == 0) == c->half_pending)
+      return fail(DG_ERR_STATE, half == 0 ? "velocity half again before the stress half" : "stress half without the velocity half");
+    if (half == 0 && c->t + 1 > c->max_steps) return fail(DG_ERR_STATE, "stepping past the end of the wavelet table");
+  }
+  CK(cudaSetDevice(c->device));
+  const bool closes = (c->part_done | part) == 3;
+  int rc = launch_part(c, half, part, closes && half == 1);
+  if (rc) return rc;
+  c->part_done |= part;
+  c->part_half = half;
+  if (closes) {
+    c->part_done = 0;
+    c->half_pending = half == 0;
+    if (half == 1) {
+      c->t += 1;
+      c->stats.steps_done = c->t;
+    }
   }
   return DG_OK;
 }
@@ -1590,12 +1668,32 @@ int dg_gpu_halo_lists(dg_gpu_ctx* c, int mesh, long n_send, const long* send, lo
   if (n_recv && (rc = c->upload(&hl.d_recv, b))) return rc;
   hl.n_send = n_send;
   hl.n_recv = n_recv;
+  if (mesh == 0 && !c->multi) {
+    // the parts of a split half step: ghosts are the received elements; the boundary part must
+    // hold every element with a ghost face neighbour (it runs after the ghosts are updated)
+    std::vector<int4> face(h.Kp);
+    const int4* d_face = c->is_double ? c->md_d[0].face : c->md_f[0].face;
+    CK(cudaMemcpyAsync(face.data(), d_face, sizeof(int4) * h.Kp, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<char> ghost(h.K, 0);
+    for (int x : b) ghost[x] = 1;
+    long eB = 0, eO = 0;
+    for (long n = 0; n < h.K; n++) {
+      if (ghost[n]) continue;
+      eO = n + 1;
+      const int codes[3] = {face[n].x, face[n].y, face[n].z};
+      for (int f = 0; f < 3; f++)
+        if (codes[f] >= 0 && ghost[codes[f] >> 4]) eB = n + 1;
+    }
+    c->part_eB = eB;
+    c->part_eO = eO;
+  }
   CK(cudaStreamSynchronize(c->stream));
   return DG_OK;
 }
 
 // what 0: the velocity planes (Vx, Vz: 12), 1: the stress planes (Txx, Tzz, Txz: 18)
-static int halo_copy(dg_gpu_ctx* c, int mesh, int what, void* buf, bool pack) {
+static int halo_copy(dg_gpu_ctx* c, int mesh, int what, void* buf, bool pack, bool sync = true) {
   if (!c || mesh < 0 || mesh >= (int)c->mi.size() || (what != 0 && what != 1))
     return fail(DG_ERR_ARG, "bad arguments");
   if ((int)c->halo.size() <= mesh) return fail(DG_ERR_STATE, "no halo lists for this mesh");
@@ -1620,11 +1718,15 @@ static int halo_copy(dg_gpu_ctx* c, int mesh, int what, void* buf, bool pack) {
     else k_halo_unpack<float><<<grid, B, 0, c->stream>>>(m.U, m.ES, m.PS, h.S, plane0, planes, el, (int)n, (const float*)buf);
   }
   CK(cudaGetLastError());
-  if (pack) CK(cudaStreamSynchronize(c->stream));
+  if (pack && sync) CK(cudaStreamSynchronize(c->stream));
   return DG_OK;
 }
 
 int dg_gpu_halo_pack(dg_gpu_ctx* c, int mesh, int what, void* buf) { return halo_copy(c, mesh, what, buf, true); }
+int dg_gpu_halo_pack_async(dg_gpu_ctx* c, int mesh, int what, void* buf) {
+  return halo_copy(c, mesh, what, buf, true, false);
+}
+void* dg_gpu_context_stream(dg_gpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
 int dg_gpu_halo_unpack(dg_gpu_ctx* c, int mesh, int what, const void* buf) {
   return halo_copy(c, mesh, what, const_cast<void*>(buf), false);
 }

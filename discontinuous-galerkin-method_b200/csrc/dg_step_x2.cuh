@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(256, 2) k_velocity_x2(const __grid_constant__ 
   const long long t = ctr->v;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
   if (t >= m.steps) return;
-  velocity_x2_body<S, KAHAN, PM>(ops, m, blockIdx.x, t);
+  velocity_x2_body<S, KAHAN, PM>(ops, m, blockIdx.x + m.block0, t);
 }
 
 // Load of a velocity value: plain, or through L2 (FRESH) when other blocks of the same launch
@@ -373,8 +373,9 @@ __global__ void __launch_bounds__(256, 2) k_stress_x2(const __grid_constant__ Op
   const long long t = ctr->s;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
   if (t >= m.steps) return;
-  if ((int)blockIdx.x >= m.n_elem_blocks) { record(m, blockIdx.x - m.n_elem_blocks, t); return; }
-  stress_x2_body<S, KAHAN, false, PM>(ops, m, blockIdx.x, t);
+  const int lb = blockIdx.x + m.block0;
+  if (lb >= m.n_elem_blocks) { record(m, lb - m.n_elem_blocks, t); return; }
+  stress_x2_body<S, KAHAN, false, PM>(ops, m, lb, t);
 }
 
 // -------------------------------------------------------------------------------------------
@@ -549,7 +550,7 @@ __global__ void __launch_bounds__(256, 2) k_velocity_x2e(const __grid_constant__
   const long long t = ctr->v;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
   if (t >= m.steps) return;
-  velocity_x2e_body<KAHAN>(ops, m, blockIdx.x, t);
+  velocity_x2e_body<KAHAN>(ops, m, blockIdx.x + m.block0, t);
 }
 
 template <bool KAHAN, bool FRESH = false>
@@ -665,8 +666,9 @@ __global__ void __launch_bounds__(256, 2) k_stress_x2e(const __grid_constant__ O
   const long long t = ctr->s;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
   if (t >= m.steps) return;
-  if ((int)blockIdx.x >= m.n_elem_blocks) { record(m, blockIdx.x - m.n_elem_blocks, t); return; }
-  stress_x2e_body<KAHAN>(ops, m, blockIdx.x, t);
+  const int lb = blockIdx.x + m.block0;
+  if (lb >= m.n_elem_blocks) { record(m, lb - m.n_elem_blocks, t); return; }
+  stress_x2e_body<KAHAN>(ops, m, lb, t);
 }
 
 }  // namespace dg

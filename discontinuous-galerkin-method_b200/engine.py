@@ -36,8 +36,11 @@ EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_tim
            "dg_gpu_fetch_traces", "dg_gpu_fetch", "dg_gpu_load",
            "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_steps_done",
            "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error", "dg_gpu_energy_noalloc",
-           "dg_gpu_debug_stall_wave", "dg_gpu_step_snapshots", "dg_gpu_half_step", "dg_gpu_halo_lists",
-           "dg_gpu_halo_pack", "dg_gpu_halo_unpack"]
+           "dg_gpu_debug_stall_wave", "dg_gpu_step_snapshots", "dg_gpu_half_step", "dg_gpu_half_step_part",
+           "dg_gpu_halo_lists", "dg_gpu_halo_pack", "dg_gpu_halo_pack_async", "dg_gpu_halo_unpack",
+           "dg_gpu_context_stream"]
+# parts of a half step (dg_gpu_half_step_part)
+PART_ALL, PART_BOUNDARY, PART_INTERIOR = 0, 1, 2
 
 
 def energy_noalloc(device: int, K: int, fields, jacobi, A, inverV: np.ndarray, out, stream=None) -> None:
@@ -125,10 +128,15 @@ def lib(path: str | None = None):
                                             C.c_void_p]
         L.dg_gpu_step_snapshots.restype = C.c_int
         L.dg_gpu_half_step.argtypes = [C.c_void_p, C.c_int]
+        L.dg_gpu_half_step_part.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.dg_gpu_halo_lists.argtypes = [C.c_void_p, C.c_int, C.c_long, C.c_void_p, C.c_long, C.c_void_p]
         L.dg_gpu_halo_pack.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.dg_gpu_halo_pack_async.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.dg_gpu_context_stream.argtypes = [C.c_void_p]
+        L.dg_gpu_context_stream.restype = C.c_void_p
         L.dg_gpu_halo_unpack.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
-        for n in ("dg_gpu_half_step", "dg_gpu_halo_lists", "dg_gpu_halo_pack", "dg_gpu_halo_unpack"):
+        for n in ("dg_gpu_half_step", "dg_gpu_half_step_part", "dg_gpu_halo_lists", "dg_gpu_halo_pack",
+                  "dg_gpu_halo_pack_async", "dg_gpu_halo_unpack"):
             getattr(L, n).restype = C.c_int
         L.dg_gpu_stats_get.argtypes = [C.c_void_p, C.c_void_p]
         L.dg_gpu_steps_done.argtypes = [C.c_void_p]
@@ -183,6 +191,7 @@ class Engine:
             meshes = [meshes]
         prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         self.precision = prec
+        self.device = int(device)
         self._keep = []
         arr = (_Mesh * len(meshes))()
         self.info = []
@@ -256,14 +265,30 @@ class Engine:
     def half_step(self, half: int):
         _check(lib().dg_gpu_half_step(self._ctx, int(half)), "dg_gpu_half_step")
 
+    def half_step_part(self, half: int, part: int):
+        """One part of a half step: PART_BOUNDARY (elements with a ghost neighbour) or
+        PART_INTERIOR (the other non-ghost elements); the half ends with its second part."""
+        _check(lib().dg_gpu_half_step_part(self._ctx, int(half), int(part)), "dg_gpu_half_step_part")
+
     def halo_lists(self, send, recv, mesh: int = 0):
         s = np.ascontiguousarray(send, dtype=np.int64)
         r = np.ascontiguousarray(recv, dtype=np.int64)
         _check(lib().dg_gpu_halo_lists(self._ctx, mesh, s.size, s.ctypes.data if s.size else None, r.size,
                                        r.ctypes.data if r.size else None), "dg_gpu_halo_lists")
 
-    def halo_pack(self, what: int, dev_ptr: int, mesh: int = 0):
-        _check(lib().dg_gpu_halo_pack(self._ctx, mesh, int(what), C.c_void_p(dev_ptr)), "dg_gpu_halo_pack")
+    def halo_pack(self, what: int, dev_ptr: int, mesh: int = 0, wait: bool = True):
+        """Pack the send list into a device buffer; `wait=False` only enqueues it on the context
+        stream (order the transfer after `stream()` with an event)."""
+        if wait:
+            _check(lib().dg_gpu_halo_pack(self._ctx, mesh, int(what), C.c_void_p(dev_ptr)), "dg_gpu_halo_pack")
+        else:
+            _check(lib().dg_gpu_halo_pack_async(self._ctx, mesh, int(what), C.c_void_p(dev_ptr)),
+                   "dg_gpu_halo_pack_async")
+
+    def stream(self):
+        """The context's CUDA stream as a `torch.cuda.ExternalStream`."""
+        import torch
+        return torch.cuda.ExternalStream(lib().dg_gpu_context_stream(self._ctx), device=self.device)
 
     def halo_unpack(self, what: int, dev_ptr: int, mesh: int = 0):
         _check(lib().dg_gpu_halo_unpack(self._ctx, mesh, int(what), C.c_void_p(dev_ptr)), "dg_gpu_halo_unpack")

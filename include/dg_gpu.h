@@ -181,6 +181,25 @@ int dg_gpu_set_wavelet(dg_gpu_ctx *ctx, int mesh, long t0, long n, const double 
  * context. */
 int dg_gpu_half_step(dg_gpu_ctx *ctx, int half);
 
+/* The same half step in two parts, so that the halo transfer overlaps computation: the boundary
+ * part holds the elements with a ghost face neighbour (it must follow the unpack of the ghosts),
+ * the interior part the other elements that are not ghosts (it needs no ghost value).  With the
+ * halo lists set (they define the parts; one-mesh contexts only), an overlapped step is
+ *     half_step_part(ctx, 0, INTERIOR)   while the previous step's stress halo is in transit
+ *     unpack stresses; half_step_part(ctx, 0, BOUNDARY); pack velocities, start their transfer
+ *     half_step_part(ctx, 1, INTERIOR)   while the velocity halo is in transit
+ *     unpack velocities; half_step_part(ctx, 1, BOUNDARY); pack stresses, start their transfer
+ * and owned elements compute exactly what dg_gpu_half_step computes, in any element numbering;
+ * the overlap is largest when the boundary elements come first (opts.reorder = 0 and a mesh
+ * numbered boundary, interior, ghosts).  Either part may run first; the half ends with the
+ * second (which records, for the stress half).  DG_PART_ALL is dg_gpu_half_step.
+ * DG_ERR_STATE if the halves do not alternate, a part runs twice or the other half's part is
+ * missing, or no halo lists are set. */
+#define DG_PART_ALL 0
+#define DG_PART_BOUNDARY 1
+#define DG_PART_INTERIOR 2
+int dg_gpu_half_step_part(dg_gpu_ctx *ctx, int half, int part);
+
 /* Elements (0-based, the mesh's own numbering) whose values this part sends, and the ghost
  * elements whose values it receives, each list in the order of the exchange buffers. */
 int dg_gpu_halo_lists(dg_gpu_ctx *ctx, int mesh, long n_send, const long *send, long n_recv, const long *recv);
@@ -190,6 +209,16 @@ int dg_gpu_halo_lists(dg_gpu_ctx *ctx, int mesh, long n_send, const long *send, 
  * [element][plane][shot] in the context's arithmetic (8-byte doubles for the FP64 precisions,
  * 4-byte floats for the FP32 ones); returns once the buffer is filled. */
 int dg_gpu_halo_pack(dg_gpu_ctx *ctx, int mesh, int what, void *buf);
+
+/* The same copy, enqueued on the context stream without waiting for it: a caller that orders
+ * its transfer after the context stream (a CUDA event recorded on dg_gpu_context_stream) and
+ * the next half step and unpack after the transfer (the context stream waiting on an event of
+ * the transfer's stream) steps a split mesh with no host synchronisation. */
+int dg_gpu_halo_pack_async(dg_gpu_ctx *ctx, int mesh, int what, void *buf);
+
+/* The context's CUDA stream (a cudaStream_t), on which every call of the context enqueues its
+ * work: for ordering the caller's own work against it with events. */
+void *dg_gpu_context_stream(dg_gpu_ctx *ctx);
 
 /* Copy a device buffer of the same layout into the planes of the receive list (enqueued on the
  * context stream, ahead of the next half step). */

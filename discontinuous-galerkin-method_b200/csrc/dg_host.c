@@ -13,6 +13,7 @@
 
 #include <fcntl.h>
 #include <math.h>
+#include <omp.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -39,10 +40,19 @@ const char *dgh_strerror(int code)
 
 /* ---------------------------------------------------------------- text numbers ---------- */
 
+/* pow(10, k) for k = -99..99 (the exponents two digits can write), filled by libm's pow itself,
+ * so a table lookup returns exactly what the reference's pow calls return. */
+typedef struct { double v[199]; } pow10_table;
+static void pow10_fill(pow10_table *t)
+{
+	for (int k = -99; k <= 99; k++) t->v[k + 99] = pow(10, k);
+}
+static inline double p10(const pow10_table *t, long k) { return (k >= -99 && k <= 99) ? t->v[k + 99] : pow(10, k); }
+
 /* ReadDouble's per-token arithmetic (fun_save_to_file.c:63-93): leading digit, then the seven
  * fraction digits added from the last one upwards with pow(10, k), then the power of ten and
  * the sign applied in that order. */
-double dgh_parse_e7(const char *s, long i)
+static double parse_e7(const char *s, long i, const pow10_table *t)
 {
 	double sign = 1.0, esign = 1.0, v;
 	long k, j, p;
@@ -50,29 +60,38 @@ double dgh_parse_e7(const char *s, long i)
 	if (s[i + 1] == '-') esign = -1.0;
 	v = (double)(s[i - 9] - '0');
 	for (j = i - 1, k = -7; j >= i - 7; j--, k++)
-		v = v + (s[j] - '0') * pow(10, k);
+		v = v + (s[j] - '0') * p10(t, k);
 	p = (long)esign * ((s[i + 2] - '0') * 10 + (s[i + 3] - '0'));
-	return v * pow(10, p) * sign;
+	return v * p10(t, p) * sign;
+}
+
+double dgh_parse_e7(const char *s, long i)
+{
+	pow10_table t;
+	pow10_fill(&t);
+	return parse_e7(s, i, &t);
 }
 
 /* ReadInt's per-token arithmetic (fun_save_to_file.c:157-185): the signed leading digit times
  * 10^p, then `p` further digits added as positive integer places.  (A negative number with
  * more than one significant digit therefore comes out wrong in the reference; -1, the only
  * negative value the mesh files hold, is exact.) */
-static long parse_int_e7(const char *s, long i)
+static long parse_int_e7(const char *s, long i, const pow10_table *t)
 {
 	long sign = 1, esign = 1, p, j, k, v;
 	if (s[i - 10] == '-') sign = -1;
 	if (s[i + 1] == '-') esign = -1;
 	p = esign * ((s[i + 2] - '0') * 10 + (s[i + 3] - '0'));
-	v = (long)((s[i - 9] - '0') * pow(10, p) * sign);
+	v = (long)((s[i - 9] - '0') * p10(t, p) * sign);
 	for (j = i - 7, k = p - 1; j <= i - 7 + p - 1; j++, k--)
-		v = (long)(v + (s[j] - '0') * pow(10, k));
+		v = (long)(v + (s[j] - '0') * p10(t, k));
 	return v;
 }
 
 void dgh_quantize_e7(double *x, long n)
 {
+	pow10_table t;
+	pow10_fill(&t);
 #pragma omp parallel for schedule(static)
 	for (long q = 0; q < n; q++) {
 		char buf[64];
@@ -81,23 +100,26 @@ void dgh_quantize_e7(double *x, long n)
 		char *e = strchr(buf + 8, 'e');
 		if (len <= 0 || !e || e - buf < 10 || !isfinite(x[q]))
 			continue;
-		x[q] = dgh_parse_e7(buf, (long)(e - buf));
+		x[q] = parse_e7(buf, (long)(e - buf), &t);
 	}
 }
 
-static char *slurp(const char *path, long *len)
+/* The file (or its first `limit` bytes, limit > 0), with 16 bytes of padding on each side so
+ * s[i-10] and s[i+3] are always addressable. */
+static char *slurp(const char *path, long *len, long limit)
 {
 	int fd = open(path, O_RDONLY);
 	if (fd < 0) return NULL;
 	struct stat st;
 	if (fstat(fd, &st) != 0) { close(fd); return NULL; }
-	/* 16 bytes of leading padding so s[i-10] is always addressable */
-	char *buf = malloc((size_t)st.st_size + 32);
+	long size = (long)st.st_size;
+	if (limit > 0 && size > limit) size = limit;
+	char *buf = malloc((size_t)size + 32);
 	if (!buf) { close(fd); return NULL; }
 	memset(buf, ' ', 16);
 	long got = 0;
-	while (got < st.st_size) {
-		ssize_t r = read(fd, buf + 16 + got, (size_t)(st.st_size - got));
+	while (got < size) {
+		ssize_t r = read(fd, buf + 16 + got, (size_t)(size - got));
 		if (r <= 0) break;
 		got += r;
 	}
@@ -108,29 +130,89 @@ static char *slurp(const char *path, long *len)
 }
 
 /* Token scan shared by both readers: every 'e' marks a number; '\n' starts a new row (the
- * reference's m/n bookkeeping, fun_save_to_file.c:95-108). */
+ * reference's m/n bookkeeping, fun_save_to_file.c:95-108); the scan stops at the wanted count.
+ * The text is cut into `C` chunks that start at line starts; a first pass counts each chunk's
+ * tokens and line breaks, so every token's ordinal and row are known and the chunks are parsed
+ * in parallel, with the checks and values of the sequential scan.  A row with more than `cols`
+ * numbers writes into the next row's slots, where the sequential scan lets the later value win:
+ * if any row does that, the caller scans again with one chunk (DGH_RESCAN). */
+#define DGH_RESCAN (-1000)
+static long scan_tokens(const char *s, long len, long rows, long cols, double *outd, long *outl, int C)
+{
+	const long want = rows * cols;
+	pow10_table t;
+	pow10_fill(&t);
+	long *cut = malloc(sizeof(long) * (size_t)(3 * C + 3));
+	if (!cut) return DGH_ERR_NOMEM;
+	long *tok0 = cut + C + 1, *row0 = tok0 + C + 1;
+	for (int c = 0; c <= C; c++) {
+		long at = len * c / C;
+		while (c > 0 && c < C && at < len && s[at - 1] != '\n') at++;
+		cut[c] = at;
+	}
+	tok0[0] = row0[0] = 0;
+#pragma omp parallel for schedule(static)
+	for (int c = 0; c < C; c++) {
+		long ne = 0, nl = 0;
+		for (long i = cut[c]; i < cut[c + 1]; i++) {
+			ne += s[i] == 'e';
+			nl += s[i] == '\n';
+		}
+		tok0[c + 1] = ne;
+		row0[c + 1] = nl;
+	}
+	for (int c = 0; c < C; c++) {
+		tok0[c + 1] += tok0[c];
+		row0[c + 1] += row0[c];
+	}
+	int bad = 0, spill = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad, spill)
+	for (int c = 0; c < C; c++) {
+		long num = tok0[c], m = row0[c], n = 0;
+		for (long i = cut[c]; i < cut[c + 1] && num < want && !bad; i++) {
+			if (s[i] == 'e') {
+				const long at = m * cols + n;
+				if (i + 3 >= len || i < 9 || s[i - 8] != '.' || at >= want) {
+					bad = 1;
+					break;
+				}
+				spill |= n >= cols;
+				if (outd) outd[at] = parse_e7(s, i, &t);
+				else outl[at] = parse_int_e7(s, i, &t);
+				n++;
+				num++;
+			}
+			if (s[i] == '\n') { m++; n = 0; }
+		}
+	}
+	const long total = tok0[C];
+	free(cut);
+	if (spill && C > 1) return DGH_RESCAN;
+	if (bad) return DGH_ERR_FORMAT;
+	return total >= want ? want : DGH_ERR_FORMAT;
+}
+
 static long read_tokens(const char *path, long rows, long cols, double *outd, long *outl)
 {
 	if (!path || rows <= 0 || cols <= 0 || (!outd && !outl)) return DGH_ERR_ARG;
 	long len;
-	char *buf = slurp(path, &len);
-	if (!buf) return DGH_ERR_IO;
-	const char *s = buf + 16;
-	long want = rows * cols, num = 0, m = 0, n = 0;
-	for (long i = 0; i < len && num < want; i++) {
-		if (s[i] == 'e') {
-			if (i + 3 >= len || i < 9 || s[i - 8] != '.') { free(buf); return DGH_ERR_FORMAT; }
-			long at = m * cols + n;
-			if (at >= want) { free(buf); return DGH_ERR_FORMAT; }
-			if (outd) outd[at] = dgh_parse_e7(s, i);
-			else outl[at] = parse_int_e7(s, i);
-			n++;
-			num++;
+	char *buf = NULL;
+	if (rows * cols == 1) {
+		/* a header value: the first line is enough, unless the first number runs past it */
+		buf = slurp(path, &len, 4096);
+		if (!buf) return DGH_ERR_IO;
+		const char *e = memchr(buf + 16, 'e', (size_t)len);
+		if (len == 4096 && (!e || e - (buf + 16) + 3 >= len)) {
+			free(buf);
+			buf = NULL;
 		}
-		if (s[i] == '\n') { m++; n = 0; }
 	}
+	if (!buf) buf = slurp(path, &len, 0);
+	if (!buf) return DGH_ERR_IO;
+	long r = scan_tokens(buf + 16, len, rows, cols, outd, outl, len < (1L << 20) ? 1 : 4 * omp_get_max_threads());
+	if (r == DGH_RESCAN) r = scan_tokens(buf + 16, len, rows, cols, outd, outl, 1);
 	free(buf);
-	return num == want ? num : DGH_ERR_FORMAT;
+	return r;
 }
 
 long dgh_read_matrix(const char *path, double *out, long rows, long cols)

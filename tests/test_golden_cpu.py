@@ -170,3 +170,51 @@ def test_host_setup_independent_of_thread_count():
         assert r.returncode == 0, r.stderr[-2000:]
         out.append(r.stdout.strip())
     assert out[0] == out[1] and len(out[0]) == 40
+
+
+def test_large_text_files_parallel_reader(tmp_path):
+    """Files above 1 MB are parsed in parallel chunks cut at line starts: integers and doubles
+    come back exactly as the sequential ReadInt/ReadDouble scan gives them, a row with one number
+    too many (it spills into the next row's first slot, which the next row then overwrites) reads
+    as the sequential scan reads it, and a missing number is a format error."""
+    import ctypes as C
+
+    rng = np.random.default_rng(7)
+    rows, cols = 60000, 3
+    ints = rng.integers(-1, 10**6, size=(rows, cols)).astype(np.int64)
+    ints[ints < 0] = -1                                   # -1 is the only negative the files hold
+    path = str(tmp_path / "ints.txt")
+    lines = ["".join("%16.7e" % v for v in r) for r in ints]
+    lines[123] += "%16.7e" % 5.0                          # one number too many in row 123
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    assert os.path.getsize(path) > (1 << 20)
+    out = np.zeros(rows * cols, dtype=np.int64)
+    assert host.lib().dgh_read_int_matrix(path.encode(), out.ctypes.data, rows, cols) == rows * cols
+    # the sequential scan, restated: slot row * cols + n, stop at the wanted count
+    want = np.zeros(rows * cols, dtype=np.int64)
+    num = 0
+    for m, line in enumerate(lines):
+        for n, tok in enumerate(line.split()):
+            if num == rows * cols:
+                break
+            want[m * cols + n] = int(float(tok))
+            num += 1
+    assert np.array_equal(out, want)
+    assert want[-1] == 0 and np.array_equal(want[:-1], ints.ravel()[:-1])   # the extra number took the last slot's turn
+
+    vals = rng.normal(size=(rows, cols)) * 10.0 ** rng.integers(-5, 6, size=(rows, cols))
+    dpath = str(tmp_path / "doubles.txt")
+    pkg.meshgen._save_ascii(dpath, vals)
+    got = np.zeros(rows * cols)
+    assert host.lib().dgh_read_matrix(dpath.encode(), got.ctypes.data, rows, cols) == rows * cols
+    parse = host.lib().dgh_parse_e7
+    parse.restype, parse.argtypes = C.c_double, [C.c_char_p, C.c_long]
+    toks = [" " * 16 + "%16.7e" % v for v in vals.ravel()[:2000]]
+    want = np.array([parse(t.encode(), t.index("e")) for t in toks])
+    assert np.array_equal(got[:2000], want)
+    assert np.allclose(got, vals.ravel(), rtol=1e-7, atol=0)
+    short = str(tmp_path / "short.txt")
+    with open(short, "w") as f:
+        f.write("\n".join(lines[:-1]) + "\n")
+    assert host.lib().dgh_read_int_matrix(short.encode(), out.ctypes.data, rows, cols) < 0

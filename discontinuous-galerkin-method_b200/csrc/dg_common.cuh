@@ -112,6 +112,17 @@ template <class R> struct MeshDev {
 // kernel writes only the counter the other one reads, so a captured graph can be replayed.
 struct Counters { long long v, s; };
 
+// gpu-scope acquire load / release store of a flag, and a volatile load of an error word
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_volatile_i32(const int* p) { return *(volatile const int*)p; }
+
 template <class R> __device__ __forceinline__ R ldg(const R* p) { return __ldg(p); }
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 __device__ __forceinline__ double4 ld4(const double4* p) {

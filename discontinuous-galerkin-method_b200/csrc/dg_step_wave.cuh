@@ -45,16 +45,6 @@ struct Wave {
   unsigned int* ptk;      // persistent form: [0] next ticket of the step, [1] blocks finished
 };
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ int ld_volatile_i32(const int* p) { return *(volatile const int*)p; }
-
 // Receivers of unit u right after its velocity update (Record, OpenMP_Function.c:61-72): each
 // thread stores the two shots it has just updated, so it reads back only its own stores.
 template <int S>

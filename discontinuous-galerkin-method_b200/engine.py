@@ -90,11 +90,13 @@ KERNEL_FAMILIES = {0: "reference operators (k_velocity_ref/k_stress_ref)",
                    5: "wavefront step: one launch per step, two shots per thread, L2-resident lag (k_step_wave)",
                    6: "wavefront step on resident blocks looping over tickets: one launch per step, two shots "
                       "per thread, L2-resident lag (k_step_wave_p)",
-                7: "two shots per thread, packed FP32x2, plane-major layout (k_velocity_x2/k_stress_x2)"}
+                   7: "two shots per thread, packed FP32x2, plane-major layout (k_velocity_x2/k_stress_x2)",
+                   8: "batch of meshes in one persistent cooperative launch, grid barrier between the halves "
+                      "(k_step_mx_p)"}
 KERNEL_NAMES = {0: ("k_velocity_ref", "k_stress_ref"), 1: ("k_velocity", "k_stress"),
                 2: ("k_velocity_x2", "k_stress_x2"), 3: ("k_velocity_x2e", "k_stress_x2e"),
                 4: ("k_velocity_mx", "k_stress_mx"), 5: ("k_step_wave", None),
-                6: ("k_step_wave_p", None), 7: ("k_velocity_x2", "k_stress_x2")}
+                6: ("k_step_wave_p", None), 7: ("k_velocity_x2", "k_stress_x2"), 8: ("k_step_mx_p", None)}
 
 
 _LIB = None

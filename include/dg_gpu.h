@@ -93,7 +93,8 @@ typedef struct {
 	int reorder;         /* 1: renumber elements along a Hilbert curve of centroids for locality */
 	int block_threads;   /* threads per block, 0: automatic (or autotuned) */
 	int graph_steps;     /* steps per captured CUDA graph, 0: automatic, <0: no graphs */
-	int autotune;        /* 1: time candidate block sizes at init */
+	int autotune;        /* 1: time candidate block sizes (and, for a batch of meshes, the persistent or
+	                        two-launch step; for the wavefront step its persistent form and lag) at init */
 	int watchdog_every;  /* check the velocity fields for NaN/Inf every k steps (0: off) */
 	const char *tune_cache; /* file that keeps autotune results between runs (NULL: none) */
 	int variant;         /* FP32 kernels: 0 automatic, 1 one (element, shot) per thread,
@@ -117,7 +118,10 @@ typedef struct {
 	                          4 FP32 batch of meshes, each block running its mesh's packed body,
 	                          5 wavefront step (one launch per step, two shots per thread, one block per ticket),
 	                          6 the same with resident blocks that loop over the tickets (FP32 default),
-	                          7 two shots per thread on plane-major state (FP32, 3-14 shots) */
+	                          7 two shots per thread on plane-major state (FP32, 3-14 shots),
+	                          8 FP32 batch of meshes in one persistent cooperative launch for many steps,
+	                            the bodies of 4 with a grid barrier between the halves (default for
+	                            batches of at least 16 work blocks per resident block) */
 } dg_gpu_stats;
 
 void dg_gpu_default_opts(dg_gpu_opts *opts);

@@ -1,0 +1,76 @@
+"""The FP32 batch of meshes in one persistent cooperative launch (`k_step_mx_p`, family 8)
+against two launches per step (`k_velocity_mx` / `k_stress_mx`, family 4).
+
+Every work block runs the same body in both forms and a grid barrier separates the halves, so
+fields and traces are equal bit for bit: stepped in one call or in chunks, timed, with
+snapshots, and after the autotuner chose between the two.  The meshes differ in shot count (the
+one-element-pair, one-(element, shot), element-major and plane-major packed bodies) and in step
+count (a mesh past its last step does nothing).
+"""
+import numpy as np
+import pytest
+
+from conftest import pkg
+
+eng = pkg.engine
+pytestmark = pytest.mark.gpu
+FIELDS = ("Vx", "Vz", "Txx", "Tzz", "Txz")
+SPEC = ((12, 150, 1), (16, 120, 2), (10, 90, 3), (14, 150, 16), (9, 150, 6))
+
+
+@pytest.fixture(scope="module")
+def meshes():
+    out = []
+    for n_cells, steps, shots in SPEC:
+        w = pkg.workloads.small_square(n_cells=n_cells, steps=steps, shots=shots)
+        out.append(eng.mesh_from_setup(pkg.host.build_setup(w, full=False), with_ref_ops=False))
+    return out
+
+
+def _run(meshes, monkeypatch, precision, persistent, chunks=(150,), timed=False, **kw):
+    monkeypatch.setenv("DG_MX_PERSISTENT", "1" if persistent else "0")
+    with eng.Engine(meshes, precision, **kw) as e:
+        fam = e.stats()["kernel_family"]
+        for c in chunks:
+            (e.step_timed if timed else e.step)(c)
+        assert e.steps_done == sum(chunks)
+        fields = [e.fetch(f, k, m) for k, (_, _, S) in enumerate(SPEC) for m in range(S) for f in FIELDS]
+        traces = [e.fetch_traces(0, steps, mesh=k) for k, (_, steps, _) in enumerate(SPEC)]
+    return fam, fields, traces
+
+
+def _same(a, b):
+    for x, y in zip(a[1], b[1]):
+        assert np.array_equal(x, y)
+    for (x0, z0), (x1, z1) in zip(a[2], b[2]):
+        assert np.array_equal(x0, x1) and np.array_equal(z0, z1)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp32_kahan"])
+def test_persistent_batch_equals_two_launches(meshes, monkeypatch, precision):
+    two = _run(meshes, monkeypatch, precision, False)
+    one = _run(meshes, monkeypatch, precision, True)
+    assert two[0] == 4 and one[0] == 8
+    assert np.abs(one[2][0][1]).max() > 0
+    _same(two, one)
+
+
+def test_persistent_batch_in_chunks_timed_and_block_sizes(meshes, monkeypatch):
+    ref = _run(meshes, monkeypatch, "fp32", False)
+    _same(ref, _run(meshes, monkeypatch, "fp32", True, chunks=(1, 7, 42, 100)))
+    _same(ref, _run(meshes, monkeypatch, "fp32", True, chunks=(3, 147), timed=True))
+    for b in (128, 256):
+        _same(ref, _run(meshes, monkeypatch, "fp32", True, block_threads=b))
+
+
+def test_persistent_batch_snapshots_and_autotune(meshes, monkeypatch):
+    ref = _run(meshes, monkeypatch, "fp32", False)
+    monkeypatch.setenv("DG_MX_PERSISTENT", "1")
+    seen = []
+    with eng.Engine(meshes, "fp32") as e:
+        e.step_snapshots(150, 50, lambda step, vx, vz: seen.append((step, vx.copy())), mesh=3, shot=5)
+        assert [s for s, _ in seen] == [50, 100, 150]
+        assert np.array_equal(seen[-1][1].ravel(), ref[1][(1 + 2 + 3) * 5 + 5 * 5])
+    tuned = _run(meshes, monkeypatch, "fp32", True, autotune=True)
+    assert tuned[0] in (4, 8)
+    _same(ref, tuned)

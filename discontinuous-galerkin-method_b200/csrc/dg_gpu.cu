@@ -123,6 +123,7 @@ struct dg_gpu_ctx {
   // launches a step; its grid, barrier words and error word
   bool mx_persistent = false;
   int blocks_mxp = 0;
+  unsigned mx_extra = 0, mx_spin = 1u << 22;  // barrier arrivals beyond the grid, poll limit
   unsigned* d_mxbar = nullptr;
   int* d_mxerr = nullptr;
   bool x2pm = false; // the two-shot bodies on the plane-major layout (MeshDev::kind 3)
@@ -893,7 +894,7 @@ int mx_resident(dg_gpu_ctx* c) {
 // nsteps steps of the FP32 batch in one cooperative launch (all blocks resident, as the grid
 // barrier needs)
 int launch_mx_p(dg_gpu_ctx* c, int nsteps) {
-  MxLoop L{c->d_btab_v, c->d_btab_t, c->blocks_v, c->blocks_t, c->d_mxbar, c->d_mxerr, 1u << 22};
+  MxLoop L{c->d_btab_v, c->d_btab_t, c->blocks_v, c->blocks_t, c->d_mxbar, c->d_mxerr, c->mx_spin, c->mx_extra};
   CK(cudaMemsetAsync(c->d_mxbar, 0, sizeof(unsigned), c->stream));
   const MeshDev<float>* tab = c->d_tab_f;
   void* args[] = {&c->ops_f, &c->ops2, &tab, &L, &c->d_ctr, &nsteps};
@@ -1804,6 +1805,11 @@ int dg_gpu_halo_unpack(dg_gpu_ctx* c, int mesh, int what, const void* buf) {
 
 int dg_gpu_debug_stall_wave(dg_gpu_ctx* c, int unit) {
   if (!c) return fail(DG_ERR_ARG, "null context");
+  if (c->mx_persistent) {  // the grid barrier waits for one arrival more than the grid holds
+    c->mx_extra = unit >= 0 ? 1u : 0u;
+    c->mx_spin = unit >= 0 ? (1u << 14) : (1u << 22);
+    return DG_OK;
+  }
   if (!c->wave) return fail(DG_ERR_UNSUPPORTED, "this context has no wavefront step");
   if (unit >= c->wv.NU) return fail(DG_ERR_ARG, "unit out of range");
   CK(cudaSetDevice(c->device));

@@ -126,6 +126,7 @@ struct MxLoop {
   unsigned* bar;       // [0] arrivals, [1] generation (arrivals zero at launch)
   int* error;
   unsigned spin_limit;
+  unsigned extra;      // arrivals expected beyond the grid: 0 (1 only in a test that makes the wait run out)
 };
 
 __device__ __forceinline__ bool grid_barrier(const MxLoop& L) {
@@ -135,7 +136,7 @@ __device__ __forceinline__ bool grid_barrier(const MxLoop& L) {
     int ok = 1;
     const unsigned gen = ld_acquire_u32(L.bar + 1);
     __threadfence();
-    if (atomicAdd(L.bar, 1u) == gridDim.x - 1) {
+    if (atomicAdd(L.bar, 1u) == gridDim.x - 1 + L.extra) {
       L.bar[0] = 0u;
       st_release_u32(L.bar + 1, gen + 1u);
     } else {

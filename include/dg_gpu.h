@@ -34,7 +34,7 @@ extern "C" {
 #define DG_ERR_UNSUPPORTED -7  /* Np != 6, Nfp != 3, more meshes than supported */
 #define DG_ERR_NODEVICE -8     /* no CUDA device, or not an sm_100 device */
 #define DG_ERR_ORIENTATION -9  /* a triangle with non-positive Jacobian (compact paths need CCW) */
-#define DG_ERR_TIMEOUT -10     /* a wait between blocks of a wavefront step reached its limit */
+#define DG_ERR_TIMEOUT -10     /* a wait between blocks (wavefront step, grid barrier of a persistent batch) reached its limit */
 
 /* arithmetic of the time loop */
 #define DG_FP64_REF 0    /* the reference's per-element Dx/Dz/Q/A/B arrays, its operation order,
@@ -248,8 +248,10 @@ int dg_gpu_flush_l2(dg_gpu_ctx *ctx);
 /* Test hook of the wavefront step (no counterpart in the reference): unit >= 0 makes the stress
  * update of that warp unit wait on a flag no warp ever publishes, so its wait reaches its limit
  * (about a second) and the next dg_gpu_step returns DG_ERR_TIMEOUT, the state of that step being
- * wrong; unit < 0 undoes it.  dg_gpu_reset then gives a context that steps as a fresh one.
- * DG_ERR_UNSUPPORTED when the context has no wavefront step. */
+ * wrong; unit < 0 undoes it.  dg_gpu_reset then gives a context that steps as a fresh one.  On a
+ * persistent batch of meshes (kernel family 8) unit >= 0 makes its grid barrier wait for one
+ * block more than the grid holds, with a short limit (milliseconds), to the same effect.
+ * DG_ERR_UNSUPPORTED when the context has neither. */
 int dg_gpu_debug_stall_wave(dg_gpu_ctx *ctx, int unit);
 
 /* Largest mesh dg_gpu_energy_noalloc accepts: its scratch holds one partial sum per 256 elements. */

@@ -74,3 +74,23 @@ def test_persistent_batch_snapshots_and_autotune(meshes, monkeypatch):
     tuned = _run(meshes, monkeypatch, "fp32", True, autotune=True)
     assert tuned[0] in (4, 8)
     _same(ref, tuned)
+
+
+def test_persistent_batch_barrier_limit_reports_timeout(meshes, monkeypatch):
+    """A grid barrier whose wait runs out (the test hook makes it wait for one block more than
+    the grid holds) ends the launch with DG_ERR_TIMEOUT; after a reset the context steps exactly
+    as a fresh one."""
+    ref = _run(meshes, monkeypatch, "fp32", False)
+    monkeypatch.setenv("DG_MX_PERSISTENT", "1")
+    with eng.Engine(meshes, "fp32") as e:
+        e.step(5)
+        e.debug_stall_wave(0)
+        with pytest.raises(eng.DGError) as ei:
+            e.step(3)
+        assert ei.value.code == -10
+        e.debug_stall_wave(-1)
+        e.reset()
+        e.step(150)
+        fields = [e.fetch(f, k, m) for k, (_, _, S) in enumerate(SPEC) for m in range(S) for f in FIELDS]
+    for x, y in zip(ref[1], fields):
+        assert np.array_equal(x, y)

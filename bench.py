@@ -50,8 +50,8 @@ def pkg():
     return importlib.import_module("discontinuous-galerkin-method_b200")
 
 
-def _uneven(steps, rank):
-    ws, _ = pkg().workloads.uneven_batch(seed=5 + 97 * rank)
+def _uneven(steps, rank, n_meshes=48):
+    ws, _ = pkg().workloads.uneven_batch(n_meshes=n_meshes, seed=5 + 97 * rank)
     for w in ws:
         w.steps = steps
     return ws
@@ -68,6 +68,9 @@ WORKLOADS = {
     "square": (lambda steps, rank: pkg().workloads.homogeneous_square(steps=steps),
                "homogeneous square: 20,000 triangles, 1 shot"),
     "uneven": (_uneven, "uneven batch: 48 meshes, 5,000-500,000 triangles (log-uniform), 1-8 shots each"),
+    # the first 12 meshes of that batch: a smaller case of the same kernels, for profiling
+    "uneven12": (lambda steps, rank: _uneven(steps, rank, 12),
+                 "uneven batch: 12 meshes, 5,000-500,000 triangles (log-uniform), 1-8 shots each"),
 }
 
 

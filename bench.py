@@ -373,18 +373,35 @@ def run_ours(args):
             cuts.append(sum(a.size for a in out))
         return np.concatenate(out), cuts
 
+    # energy (FP64 sums on the device) of up to 8 (mesh, shot) pairs, every quarter of the run
+    pairs = [(k, m) for k, x in enumerate(ws) for m in range(x.shots)]
+    pairs = pairs[:: max(1, len(pairs) // 8)][:8]
+    quarters = 4
+
+    def run_accuracy(engine):
+        energy = []
+        for _ in range(quarters):
+            engine.step(acc_steps // quarters)
+            energy.append([engine.fetch("energy", k, m) for k, m in pairs])
+        return np.array(energy)
+
     e.reset()
-    e.step(acc_steps)
+    en = run_accuracy(e)
     tr, cuts = traces(e)
     e.close()
     accuracy = None
     if args.precision != "fp64":
         with eng.Engine(meshes, "fp64", device=device) as e64:
-            e64.step(acc_steps)
+            en64 = run_accuracy(e64)
             tr64, _ = traces(e64)
+        drift = [float(np.abs(en[:, j] - en64[:, j]).max() / en64[:, j].max())
+                 for j in range(len(pairs)) if en64[:, j].max() > 0]
+        energy_acc = {"energy_rel_vs_fp64": max(drift) if drift else None,
+                      "energy_what": "max over t of |E(t) - E_fp64(t)| / max E_fp64, %d (mesh, shot) pairs, "
+                                     "every %d steps" % (len(pairs), acc_steps // quarters)}
         if np.linalg.norm(tr64) > 0:
             accuracy = {"trace_rel_l2_vs_fp64": float(np.linalg.norm(tr - tr64) / np.linalg.norm(tr64)),
-                        "steps": acc_steps, "shots": S_tot}
+                        "steps": acc_steps, "shots": S_tot, **energy_acc}
             if len(ws) > 1:
                 # each mesh on its own; None where the wave has not reached a receiver yet (its FP64
                 # traces hold only the numerical precursor, below 1e-10 of the batch's largest
@@ -401,7 +418,7 @@ def run_ours(args):
                 accuracy["per_mesh_note"] = ("None: no arrival at a receiver in these steps (FP64 traces "
                                              "below 1e-10 of the batch maximum)")
         else:  # the wave has not reached a receiver yet: nothing to compare
-            accuracy = {"trace_rel_l2_vs_fp64": None, "steps": acc_steps, "shots": S_tot,
+            accuracy = {"trace_rel_l2_vs_fp64": None, "steps": acc_steps, "shots": S_tot, **energy_acc,
                         "note": "FP64 traces still zero after %d steps (source delay); the long-run "
                                 "accuracy of this workload is checked in tests/test_gpu_fullsize.py" % acc_steps}
 

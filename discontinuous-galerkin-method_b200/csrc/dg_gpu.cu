@@ -773,13 +773,13 @@ int build_wave(dg_gpu_ctx* c) {
 
 // shot counts with a two-shot FP32 kernel instance (element-major), and with a plane-major one
 bool x2_supported(int S) { return (S >= 2 && S <= 16 && S % 2 == 0) || S == 32 || S == 64 || S == 128; }
-bool x2pm_supported(int S) { return S >= 4 && S <= 16 && S % 2 == 0; }
+bool x2pm_supported(int S) { return S >= 2 && S <= 16 && S % 2 == 0; }
 
 // Kernel body and stored shot count for a mesh of S shots: FP32 meshes use the packed bodies —
-// two elements per thread for one shot, two shots per thread from three shots on (plane-major
-// layout up to 14 stored shots, element-major above), an odd count padded with one silent shot
-// — unless the caller asks for one (element, shot) per thread (variant 1); two shots take one
-// (element, shot) per thread unless variant 2 or 3 or the wavefront step is asked for.
+// two elements per thread for one shot, two shots per thread from two shots on (plane-major
+// layout up to 14 stored shots, element-major above or for the wavefront step), an odd count
+// padded with one silent shot — unless the caller asks for one (element, shot) per thread
+// (variant 1).
 void choose_kind(int S, long K, bool fp32, int variant, bool want_wave, int& kind, int& S_pad) {
   kind = 0;
   S_pad = S;
@@ -788,16 +788,14 @@ void choose_kind(int S, long K, bool fp32, int variant, bool want_wave, int& kin
     kind = 1;
     return;
   }
-  // two shots: one (element, shot) per thread unless asked otherwise.  The packed body would
-  // give each thread a whole element, so a warp's loads scatter over 32 element records
-  // (200k elements: 245 G DOF-updates/s against 163 G; from 4 shots on the packed body wins)
-  if (S == 2 && variant != 2 && variant != 3 && !want_wave) return;
   const int even = S + (S & 1);
   if (x2_supported(even) && (long long)K * (even / 2) < (1LL << 31)) {
-    // plane-major packed body for 4..14 stored shots: the element-major one scatters a warp's
+    // plane-major packed body for 2..14 stored shots: the element-major one scatters a warp's
     // loads over a few element records (200k elements, two launches: 4 shots 333 G against
-    // 269 G DOF-updates/s, 6: 357 against 284, 8: 382 against 358, 16: equal); the wavefront
-    // step needs the element-major layout
+    // 269 G DOF-updates/s, 6: 357 against 284, 8: 382 against 358, 16: equal; at two shots it
+    // gives each thread a whole element record, 163 G, below one (element, shot) per thread,
+    // 248 G, while the plane-major body runs at 319 G, and 405 G against 276 G on 2M elements);
+    // the wavefront step needs the element-major layout
     const bool pm = x2pm_supported(even) && (variant == 3 || (variant == 0 && !want_wave && even <= 14));
     kind = pm ? 3 : 2;
     S_pad = even;
@@ -827,7 +825,7 @@ int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid, bool hv = true, bool ht = true) {
     if (ht) k_stress_x2<SS, KAHAN, true><<<gt, bl, 0, st>>>(c->ops2, c->md_f[0], c->d_ctr);   \
     break;
     DG_X2(2) DG_X2(4) DG_X2(6) DG_X2(8) DG_X2(10) DG_X2(12) DG_X2(14) DG_X2(16) DG_X2(32) DG_X2(64) DG_X2(128)
-    DG_X2PM(4) DG_X2PM(6) DG_X2PM(8) DG_X2PM(10) DG_X2PM(12) DG_X2PM(14) DG_X2PM(16)
+    DG_X2PM(2) DG_X2PM(4) DG_X2PM(6) DG_X2PM(8) DG_X2PM(10) DG_X2PM(12) DG_X2PM(14) DG_X2PM(16)
 #undef DG_X2PM
 #undef DG_X2
     default:

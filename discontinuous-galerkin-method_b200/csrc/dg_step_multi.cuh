@@ -13,7 +13,7 @@ namespace dg {
 
 #define DG_MX_SHOTS(CALL) \
   CALL(2) CALL(4) CALL(6) CALL(8) CALL(10) CALL(12) CALL(14) CALL(16) CALL(32) CALL(64) CALL(128)
-#define DG_MX_PM_SHOTS(CALL) CALL(4) CALL(6) CALL(8) CALL(10) CALL(12) CALL(14) CALL(16)
+#define DG_MX_PM_SHOTS(CALL) CALL(2) CALL(4) CALL(6) CALL(8) CALL(10) CALL(12) CALL(14) CALL(16)
 
 // The velocity half of one block of the batch: block lb of mesh m, in the body of its kind.
 template <bool KAHAN>

@@ -99,7 +99,7 @@ typedef struct {
 	const char *tune_cache; /* file that keeps autotune results between runs (NULL: none) */
 	int variant;         /* FP32 kernels: 0 automatic, 1 one (element, shot) per thread,
 	                        2 packed FP32x2 kernels (two elements or two shots per thread; element-major
-	                        state for two shots per thread), 3 the same with plane-major state for 4-16 shots */
+	                        state for two shots per thread), 3 the same with plane-major state for 2-16 shots */
 	int wavefront;       /* one launch per step that keeps the state in flight in L2 (single FP32 mesh
 	                        of 1, 2, 4, ..., 128 shots): 0 automatic (on from 16 shots), 1 on, -1 off */
 } dg_gpu_opts;
@@ -118,7 +118,7 @@ typedef struct {
 	                          4 FP32 batch of meshes, each block running its mesh's packed body,
 	                          5 wavefront step (one launch per step, two shots per thread, one block per ticket),
 	                          6 the same with resident blocks that loop over the tickets (FP32 default),
-	                          7 two shots per thread on plane-major state (FP32, 3-14 shots),
+	                          7 two shots per thread on plane-major state (FP32, 2-14 shots),
 	                          8 FP32 batch of meshes in one persistent cooperative launch for many steps,
 	                            the bodies of 4 with a grid barrier between the halves (default for
 	                            batches of at least 16 work blocks per resident block) */

@@ -185,22 +185,32 @@ def one_shot(w):
     return pkg().workloads.Workload(w.name, w.mesh, w.vp, w.vs, w.rho, w.fp, w.sponge, w.src[:1], w.rec, w.steps)
 
 
+REF_BUILDS = {True: "throughput build -O3 -march=x86-64-v3 (no FP contraction: the parity build's bits)",
+              False: "parity build -O2"}
+
+
 def cpu_reference(w, steps_hint: float = 12.0):
-    """Time the reference's own OpenMP code (oracle/_ref) on this host: one shot, all cores."""
+    """Time the reference's own OpenMP code (oracle/_ref, its throughput build where this host
+    runs it) on this host: one shot, all cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refrun  # CPU-baseline leg only
 
     cores = os.cpu_count() or 1
     w1 = one_shot(w)
-    if refrun.available(w1):
+    fast = refrun.available(w1, fast=True)
+    build = ""
+    if fast or refrun.available(w1):
         with tempfile.TemporaryDirectory() as d:
-            probe = refrun.run(w1, os.path.join(d, "p"), steps=5, threads=cores, dump_setup=0, work_dir=os.path.join(d, "w"))
+            probe = refrun.run(w1, os.path.join(d, "p"), steps=5, threads=cores, dump_setup=0,
+                               work_dir=os.path.join(d, "w"), fast=fast)
             per = probe["timing"]["loop_seconds"] / 5
             n = int(max(10, min(w.steps, steps_hint / max(per, 1e-6))))
-            r = refrun.run(w1, os.path.join(d, "r"), steps=n, threads=cores, dump_setup=0, work_dir=os.path.join(d, "w"))
+            r = refrun.run(w1, os.path.join(d, "r"), steps=n, threads=cores, dump_setup=0,
+                           work_dir=os.path.join(d, "w"), fast=fast)
             sec = r["timing"]["loop_seconds"]
             th = int(r["timing"]["threads"])
         kind = "reference"
+        build = ", " + REF_BUILDS[fast]
     else:
         import oracle
         s = pkg().host.build_setup(w1, full=True, n_steps=max(w.steps, 10))
@@ -217,7 +227,7 @@ def cpu_reference(w, steps_hint: float = 12.0):
     dof = 30.0 * w1.K * n
     return {"value": dof / sec, "unit": UNIT, "cores": th, "kind": kind,
             "sample": "1 of %d shots of a %d-triangle mesh, first %d time steps, OpenMP %d threads, loop time only "
-                      "(%.1f s)" % (w.shots, w1.K, n, th, sec)}
+                      "(%.1f s)%s" % (w.shots, w1.K, n, th, sec, build)}
 
 
 def run_reference_arm(args):
@@ -231,15 +241,18 @@ def run_reference_arm(args):
     import refrun
     cores = os.cpu_count() or 1
     w1 = one_shot(w)
+    fast = refrun.available(w1, fast=True)
+    build = "the oracle port (C restatement)"
     with tempfile.TemporaryDirectory() as d:
-        if refrun.available(w1):
+        if fast or refrun.available(w1):
             if args.warmup:
                 refrun.run(w1, os.path.join(d, "w"), steps=args.warmup, threads=cores, dump_setup=0,
-                           work_dir=os.path.join(d, "in"))
+                           work_dir=os.path.join(d, "in"), fast=fast)
             r = refrun.run(w1, os.path.join(d, "t"), steps=args.steps, threads=cores, dump_setup=0,
-                           work_dir=os.path.join(d, "in"))
+                           work_dir=os.path.join(d, "in"), fast=fast)
             sec = r["timing"]["loop_seconds"]
             kind, th = "reference", int(r["timing"]["threads"])
+            build = "the reference's code, " + REF_BUILDS[fast]
         else:
             import oracle
             s = pkg().host.build_setup(w1, full=True)
@@ -255,8 +268,8 @@ def run_reference_arm(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc, "shots_timed": 1, "K": w1.K, "threads": th},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": kind,
-                             "sample": "1 shot of the first mesh, %d time steps after %d warm-up steps"
-                                       % (args.steps, args.warmup)},
+                             "sample": "1 shot of the first mesh, %d time steps after %d warm-up steps, %s"
+                                       % (args.steps, args.warmup, build)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0

@@ -21,13 +21,32 @@ meshgen = _pkg.meshgen
 operators = _pkg.operators
 
 
-def binary_for(w) -> str:
+# instruction-set features of the x86-64-v3 level the throughput build is compiled for
+_V3 = ("avx", "avx2", "bmi1", "bmi2", "f16c", "fma", "movbe", "xsave", "abm")
+
+
+def host_has_v3() -> bool:
+    """True if this host's CPU reports every x86-64-v3 feature (Linux /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    have = set(line.split(":", 1)[1].split())
+                    return all(x in have for x in _V3)
+    except OSError:
+        pass
+    return False
+
+
+def binary_for(w, fast: bool = False) -> str:
+    """The parity build, or (fast) the throughput build of the same sources and settings."""
     bx, bz, mw, mh = (int(round(v)) for v in w.sponge)
-    return os.path.join(REF_DIR, "dgref_F%d_X%d_Z%d_W%d_H%d" % (int(round(w.fp)), bx, bz, mw, mh))
+    name = "dgref_%sF%d_X%d_Z%d_W%d_H%d" % ("fast_" if fast else "", int(round(w.fp)), bx, bz, mw, mh)
+    return os.path.join(REF_DIR, name)
 
 
-def available(w) -> bool:
-    return os.access(binary_for(w), os.X_OK)
+def available(w, fast: bool = False) -> bool:
+    return os.access(binary_for(w, fast), os.X_OK) and (not fast or host_has_v3())
 
 
 def write_inputs(w, d: str, matrix_dir: str | None = None) -> dict:
@@ -45,8 +64,8 @@ def write_inputs(w, d: str, matrix_dir: str | None = None) -> dict:
 
 def run(w, out_dir: str, *, steps: int | None = None, snap_every: int = 0, threads: int = 0,
         shots_to_run: int | None = None, dump_setup: int = 1, matrix_dir: str | None = None,
-        work_dir: str | None = None, timeout: float | None = None) -> dict:
-    """Run the reference harness; returns {"timing": {...}, "out": out_dir}."""
+        work_dir: str | None = None, timeout: float | None = None, fast: bool = False) -> dict:
+    """Run the reference harness (fast: the throughput build); returns {"timing": {...}, "out": out_dir}."""
     if w.shots > 64:
         raise ValueError("the harness takes at most 64 shots")
     tmp = None
@@ -71,7 +90,7 @@ def run(w, out_dir: str, *, steps: int | None = None, snap_every: int = 0, threa
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
         env.setdefault("OMP_PROC_BIND", "close")
-        subprocess.run([binary_for(w), paths["prefix"], paths["matrix_dir"], cfg, out_dir], check=True,
+        subprocess.run([binary_for(w, fast), paths["prefix"], paths["matrix_dir"], cfg, out_dir], check=True,
                        env=env, timeout=timeout)
         timing = {}
         with open(os.path.join(out_dir, "timing.txt")) as f:

@@ -189,7 +189,7 @@ REF_BUILDS = {True: "throughput build -O3 -march=x86-64-v3 (no FP contraction: t
               False: "parity build -O2"}
 
 
-def cpu_reference(w, steps_hint: float = 12.0):
+def cpu_reference(w, steps_hint: float = 6.0):
     """Time the reference's own OpenMP code (oracle/_ref, its throughput build where this host
     runs it) on this host: one shot, all cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -204,7 +204,9 @@ def cpu_reference(w, steps_hint: float = 12.0):
             probe = refrun.run(w1, os.path.join(d, "p"), steps=5, threads=cores, dump_setup=0,
                                work_dir=os.path.join(d, "w"), fast=fast)
             per = probe["timing"]["loop_seconds"] / 5
-            n = int(max(10, min(w.steps, steps_hint / max(per, 1e-6))))
+            # steps from the early-step probe; later steps run up to 3x slower (subnormal values
+            # spread ahead of the wave front), so the sample ends near 10-30 s; at most 1,000
+            n = int(max(10, min(1000, steps_hint / max(per, 1e-6))))
             r = refrun.run(w1, os.path.join(d, "r"), steps=n, threads=cores, dump_setup=0,
                            work_dir=os.path.join(d, "w"), fast=fast)
             sec = r["timing"]["loop_seconds"]
@@ -213,12 +215,12 @@ def cpu_reference(w, steps_hint: float = 12.0):
         build = ", " + REF_BUILDS[fast]
     else:
         import oracle
-        s = pkg().host.build_setup(w1, full=True, n_steps=max(w.steps, 10))
+        s = pkg().host.build_setup(w1, full=True, n_steps=4000)
         o = oracle.Oracle.from_setup(s)
         t = time.perf_counter()
         o.run(0, 3, threads=cores, record=True)
         per = (time.perf_counter() - t) / 3
-        n = int(max(10, min(s.n_steps - 3, steps_hint / max(per, 1e-6))))
+        n = int(max(10, min(1000, s.n_steps - 3, steps_hint / max(per, 1e-6))))
         t = time.perf_counter()
         o.run(0, n, threads=cores, record=True)
         sec = time.perf_counter() - t

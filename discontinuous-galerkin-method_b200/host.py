@@ -39,6 +39,12 @@ def lib():
         _LIB.dgh_ricker.argtypes = [C.c_long, C.c_double, C.c_double, C.c_double, C.c_double]
         _LIB.dgh_write_matrix.restype = C.c_int
         _LIB.dgh_write_matrix.argtypes = [C.c_char_p, C.c_void_p, C.c_long, C.c_long]
+        _LIB.dgh_write_binary.restype = C.c_int
+        _LIB.dgh_write_binary.argtypes = [C.c_char_p, C.c_void_p, C.c_long]
+        _LIB.dgh_write_record.restype = C.c_int
+        _LIB.dgh_write_record.argtypes = [C.c_char_p, C.c_void_p, C.c_long]
+        _LIB.dgh_parse_e7.restype = C.c_double
+        _LIB.dgh_parse_e7.argtypes = [C.c_char_p, C.c_long]
     return _LIB
 
 

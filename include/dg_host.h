@@ -15,6 +15,7 @@
  *                          (fun_DG.c:122-1310; DG_leap_Frog_OpenMP.c:203-356)
  *   dgh_write_matrix       Save_Data ("%0.14f ")         fun_save_to_file.c:233-255
  *   dgh_write_record       Save_Record                   fun_save_to_file.c:260-281
+ *   dgh_write_binary       (new) the same values as raw little-endian doubles
  * Differences from the reference, all deliberate: no 100 MB input cap (fun_save_to_file.c:36);
  * every function returns a status instead of printing and carrying on or calling exit();
  * the absorbing list is used with its filled length; receivers are stored with stride 2.
@@ -121,9 +122,12 @@ int dgh_build(const dgh_setup_in *in, dgh_setup_out *out);
 /* The per-step source amplitude, Ricker_Source (fun_DG.c:1279-1286). */
 double dgh_ricker(long step, double dt, double t0, double fp, double pi);
 
-/* Text writers of fun_save_to_file.c: "%0.14f " per value, one row per line. */
+/* Text writers of fun_save_to_file.c: "%0.14f " per value, one row per line.  Rows are formatted
+ * on OpenMP threads and written in order, so the file holds the bytes of the sequential loop. */
 int dgh_write_matrix(const char *path, const double *m, long rows, long cols);
 int dgh_write_record(const char *path, const double *m, long rows);
+/* n doubles as raw bytes (a snapshot or trace dump that reads back exactly). */
+int dgh_write_binary(const char *path, const double *m, long n);
 
 const char *dgh_strerror(int code);
 

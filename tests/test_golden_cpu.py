@@ -177,8 +177,6 @@ def test_large_text_files_parallel_reader(tmp_path):
     come back exactly as the sequential ReadInt/ReadDouble scan gives them, a row with one number
     too many (it spills into the next row's first slot, which the next row then overwrites) reads
     as the sequential scan reads it, and a missing number is a format error."""
-    import ctypes as C
-
     rng = np.random.default_rng(7)
     rows, cols = 60000, 3
     ints = rng.integers(-1, 10**6, size=(rows, cols)).astype(np.int64)
@@ -209,7 +207,6 @@ def test_large_text_files_parallel_reader(tmp_path):
     got = np.zeros(rows * cols)
     assert host.lib().dgh_read_matrix(dpath.encode(), got.ctypes.data, rows, cols) == rows * cols
     parse = host.lib().dgh_parse_e7
-    parse.restype, parse.argtypes = C.c_double, [C.c_char_p, C.c_long]
     toks = [" " * 16 + "%16.7e" % v for v in vals.ravel()[:2000]]
     want = np.array([parse(t.encode(), t.index("e")) for t in toks])
     assert np.array_equal(got[:2000], want)
@@ -218,3 +215,28 @@ def test_large_text_files_parallel_reader(tmp_path):
     with open(short, "w") as f:
         f.write("\n".join(lines[:-1]) + "\n")
     assert host.lib().dgh_read_int_matrix(short.encode(), out.ctypes.data, rows, cols) < 0
+
+
+def test_text_and_binary_writers(tmp_path):
+    """Save_Data's format ("%0.14f " per value, a line break per row) from the parallel writer,
+    over several blocks of rows and with the values printf treats specially; and the binary dump
+    reads back exactly."""
+    rng = np.random.default_rng(11)
+    rows, cols = 70001, 3
+    m = rng.normal(size=(rows, cols)) * 10.0 ** rng.integers(-15, 4, size=(rows, cols))
+    m[5] = [0.0, -0.0, 1e300]
+    m[40000] = [np.inf, -np.inf, np.nan]
+    m[69999] = [-1e-300, 5e-324, -123456.78901234567]
+    path = str(tmp_path / "snap.txt")
+    assert host.lib().dgh_write_matrix(path.encode(), m.ctypes.data, rows, cols) == 0
+    want = "".join("".join("%0.14f " % v for v in r) + "\n" for r in m)
+    with open(path) as f:
+        assert f.read() == want
+    rec = m[:, 0].copy()
+    assert host.lib().dgh_write_record(path.encode(), rec.ctypes.data, rows) == 0
+    with open(path) as f:
+        assert f.read() == "".join("%0.14f \n" % v for v in rec)
+    bpath = str(tmp_path / "snap.bin")
+    assert host.lib().dgh_write_binary(bpath.encode(), m.ctypes.data, m.size) == 0
+    back = np.fromfile(bpath, dtype=np.float64).reshape(rows, cols)
+    assert np.array_equal(back, m, equal_nan=True)

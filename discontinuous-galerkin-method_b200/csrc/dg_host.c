@@ -14,6 +14,7 @@
 #include <fcntl.h>
 #include <math.h>
 #include <omp.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -726,6 +727,59 @@ fail:
 }
 
 /* Save_Data / Save_Record (fun_save_to_file.c:233-281) with a status instead of exit(0) */
+/* "%0.14f " of v into out (at least 512 bytes), returning the length.  A double is M * 2^E
+ * (M < 2^53); M * 10^14 fits in 128 bits, so v * 10^14 is that product shifted right by -E,
+ * rounded to nearest with ties to even on the bits shifted out — the correctly rounded decimal
+ * that printf writes.  Values with E > 0 (|v| >= 2^53), infinities and NaN go to snprintf; values
+ * below 2^-127 * 2^53 round to a signed zero. */
+static int format_f14(char *out, double v)
+{
+	uint64_t bits;
+	memcpy(&bits, &v, sizeof bits);
+	const int neg = (int)(bits >> 63), ex = (int)((bits >> 52) & 0x7ff);
+	const uint64_t man = bits & ((1ULL << 52) - 1);
+	if (ex == 0x7ff) return snprintf(out, 512, "%0.14f ", v);
+	const uint64_t M = ex ? man | (1ULL << 52) : man;
+	const int E = ex ? ex - 1075 : -1074;
+	if (E > 0) return snprintf(out, 512, "%0.14f ", v);
+	const unsigned __int128 P = (unsigned __int128)M * 100000000000000ULL;  /* < 2^100 */
+	const int sh = -E;
+	unsigned __int128 q = 0;
+	if (sh < 128) {
+		q = P >> sh;
+		if (sh > 0) {
+			const unsigned __int128 rem = P - (q << sh), half = (unsigned __int128)1 << (sh - 1);
+			if (rem > half || (rem == half && (q & 1))) q++;
+		}
+	}
+	uint64_t ip, fp;
+	if (q >> 64) {
+		ip = (uint64_t)(q / 100000000000000ULL);
+		fp = (uint64_t)(q % 100000000000000ULL);
+	} else {
+		const uint64_t q64 = (uint64_t)q;
+		ip = q64 / 100000000000000ULL;
+		fp = q64 % 100000000000000ULL;
+	}
+	char *o = out;
+	if (neg) *o++ = '-';
+	char digits[24];
+	int nd = 0;
+	do {
+		digits[nd++] = (char)('0' + ip % 10);
+		ip /= 10;
+	} while (ip);
+	while (nd) *o++ = digits[--nd];
+	*o++ = '.';
+	for (int k = 13; k >= 0; k--) {
+		o[k] = (char)('0' + fp % 10);
+		fp /= 10;
+	}
+	o += 14;
+	*o++ = ' ';
+	return (int)(o - out);
+}
+
 /* The rows [r0, r1) as Save_Data prints them ("%0.14f " per value, a line break per row), into
  * a growing buffer; 0 on success. */
 typedef struct { char *p; size_t len, cap; } text_buf;
@@ -735,7 +789,7 @@ static int format_rows(text_buf *b, const double *m, long r0, long r1, long cols
 	b->len = 0;
 	for (long i = r0; i < r1; i++) {
 		for (long j = 0; j <= cols; j++) {
-			int n = j < cols ? snprintf(tmp, sizeof tmp, "%0.14f ", m[i * cols + j]) : 1;
+			int n = j < cols ? format_f14(tmp, m[i * cols + j]) : 1;
 			if (j == cols) tmp[0] = '\n';
 			if (n < 0 || n >= (int)sizeof tmp) return -1;
 			if (b->len + (size_t)n > b->cap) {

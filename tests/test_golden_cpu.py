@@ -218,15 +218,20 @@ def test_large_text_files_parallel_reader(tmp_path):
 
 
 def test_text_and_binary_writers(tmp_path):
-    """Save_Data's format ("%0.14f " per value, a line break per row) from the parallel writer,
-    over several blocks of rows and with the values printf treats specially; and the binary dump
-    reads back exactly."""
+    """Save_Data's format ("%0.14f " per value, a line break per row) from the parallel writer and
+    its own exact decimal conversion, over several blocks of rows, with the values printf treats
+    specially and exact decimal ties (Python's %-formatting, like printf, is correctly rounded,
+    ties to even); and the binary dump reads back exactly."""
     rng = np.random.default_rng(11)
     rows, cols = 70001, 3
     m = rng.normal(size=(rows, cols)) * 10.0 ** rng.integers(-15, 4, size=(rows, cols))
     m[5] = [0.0, -0.0, 1e300]
     m[40000] = [np.inf, -np.inf, np.nan]
     m[69999] = [-1e-300, 5e-324, -123456.78901234567]
+    # exact decimal ties at the 14th place (odd multiples of 2^-15) round to even, as printf does
+    j = 2 * rng.integers(0, 2**30, size=(3000, cols)) + 1
+    m[1000:4000] = np.ldexp(j.astype(np.float64), -15) * np.where(rng.integers(0, 2, size=(3000, cols)), 1.0, -1.0)
+    m[4000:4100] = 10.0 ** rng.uniform(5, 15.9, size=(100, cols))   # wide integer parts, up to 2^53
     path = str(tmp_path / "snap.txt")
     assert host.lib().dgh_write_matrix(path.encode(), m.ctypes.data, rows, cols) == 0
     want = "".join("".join("%0.14f " % v for v in r) + "\n" for r in m)

@@ -3,3 +3,4 @@ from . import build, meshgen, operators, workloads  # noqa: F401
 from . import host  # noqa: F401
 from . import engine  # noqa: F401  (loads libdg_gpu.so lazily, on first use)
 from . import decompose  # noqa: F401
+from . import sharding  # noqa: F401

@@ -133,9 +133,9 @@ def test_halo_transfer_between_gloo_ranks():
     port = s.getsockname()[1]
     s.close()
     world = 3
-    mgr = mp.Manager()
-    out = mgr.dict()
     ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()  # a server process started by spawn, not fork
+    out = mgr.dict()
     procs = [ctx.Process(target=_rank_worker, args=(r, world, port, out)) for r in range(world)]
     for p in procs:
         p.start()

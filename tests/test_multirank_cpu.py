@@ -40,9 +40,9 @@ def _worker(rank, world, port, out):
 
 def test_two_ranks_weak_scaling_and_distinct_shots():
     world = 2
-    mgr = mp.Manager()
-    out = mgr.dict()
     ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()  # a server process started by spawn, not fork
+    out = mgr.dict()
     port = _free_port()
     procs = [ctx.Process(target=_worker, args=(r, world, port, out)) for r in range(world)]
     for p in procs:

@@ -79,3 +79,36 @@ def test_trace_gather_between_gloo_ranks():
         p.join(180)
         assert p.exitcode == 0
     assert all(out[r] for r in range(world))
+
+
+def _nccl_worker(port, out):
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from conftest import pkg as P
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": "0", "WORLD_SIZE": "1"})
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    local = np.arange(2 * 5 * 3, dtype=np.float64).reshape(2, 5, 3)
+    got = P.sharding.gather_traces(dist, local, root=0, device=torch.device("cuda", 0))
+    out[0] = len(got) == 1 and bool(np.array_equal(got[0], local))
+    dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_trace_gather_over_nccl_single_rank():
+    """The gather with CUDA tensors over NCCL (one rank: all this pool's calls have one GPU)."""
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    p = ctx.Process(target=_nccl_worker, args=(port, out))
+    p.start()
+    p.join(180)
+    assert p.exitcode == 0 and out[0]

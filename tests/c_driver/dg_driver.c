@@ -124,6 +124,26 @@ int main(int argc, char **argv)
 	rc = save(out, "trace_x", tx, steps * R) | save(out, "trace_z", tz, steps * R) | save(out, "Txz", txz, K * 6) |
 		 save(out, "snapshots", sn.all, sn.count * 2 * K * 6);
 	printf("steps %ld snapshots %ld family %d\n", st.steps_done, sn.count, st.kernel_family);
+
+	/* the same steps again as half steps in two parts (no ghosts here, so every element is in
+	 * the interior part), the parts in both orders, with an enqueue-only pack of the (empty)
+	 * send list on the context's stream */
+	int rp = dg_gpu_reset(ctx);
+	if (!rp && !dg_gpu_context_stream(ctx)) rp = -1;
+	if (!rp) rp = dg_gpu_halo_lists(ctx, 0, 0, NULL, 0, NULL);
+	for (long t = 0; t < steps && !rp; t++) {
+		rp = dg_gpu_half_step_part(ctx, 0, DG_PART_INTERIOR);
+		if (!rp) rp = dg_gpu_half_step_part(ctx, 0, DG_PART_BOUNDARY);
+		if (!rp) rp = dg_gpu_halo_pack_async(ctx, 0, 0, NULL);
+		if (!rp) rp = dg_gpu_half_step_part(ctx, 1, DG_PART_BOUNDARY);
+		if (!rp) rp = dg_gpu_half_step_part(ctx, 1, DG_PART_INTERIOR);
+	}
+	if (!rp) rp = dg_gpu_fetch(ctx, DG_TXZ, 0, 0, txz);
+	if (rp) {
+		fprintf(stderr, "half steps in parts: %s (%s)\n", dg_gpu_strerror(rp), dg_gpu_last_error());
+		return 1;
+	}
+	rc |= save(out, "Txz_parts", txz, K * 6);
 	dg_gpu_free(ctx);
 	return rc;
 }

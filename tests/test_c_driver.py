@@ -2,7 +2,8 @@
 
 CPU: the driver (tests/c_driver/dg_driver.c) compiles as C99 against include/dg_gpu.h with
 -Wall -Werror and links against libdg_gpu.so.  GPU: it runs on set-up arrays written by Python
-and its traces, final field and snapshots equal the Python binding's bit for bit.
+and its traces, final field and snapshots equal the Python binding's bit for bit; the same steps
+taken again as half steps in parts (dg_gpu_half_step_part) give the same field.
 """
 import os
 import shutil
@@ -53,7 +54,9 @@ def test_c_driver_equals_python_binding(tmp_path, precision):
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     K, R = s.K, s.n_rec
-    got = {n: np.fromfile(tmp_path / "out" / (n + ".bin")) for n in ("trace_x", "trace_z", "Txz", "snapshots")}
+    got = {n: np.fromfile(tmp_path / "out" / (n + ".bin"))
+           for n in ("trace_x", "trace_z", "Txz", "snapshots", "Txz_parts")}
+    assert np.array_equal(got["Txz_parts"], got["Txz"])    # the same steps as half steps in parts
     snaps = []
     with pkg.engine.Engine(mesh, precision) as e:
         for _ in range(5):

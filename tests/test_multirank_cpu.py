@@ -8,7 +8,6 @@ import os
 import socket
 import sys
 
-import numpy as np
 import pytest
 import torch.multiprocessing as mp
 

@@ -63,10 +63,10 @@ __global__ void k_fetch_trace(const R* __restrict__ tr, int comp, int n_rec, int
   out[q] = (double)tr[((t * 2 + comp) * n_rec + r) * (long long)S + s];
 }
 
-// traces of steps [t0, t0+n) of the first S_out shots (of S_lay stored) -> out[comp][s][t - t0][r]
+// traces of steps [t0, t0+n) of the first S_out shots (of S_lay stored) -> out_x / out_z [s][t - t0][r]
 template <class R>
 __global__ void k_fetch_traces(const R* __restrict__ tr, int n_rec, int S_lay, int S_out, long long t0, long long n,
-                               double* __restrict__ out) {
+                               double* __restrict__ out_x, double* __restrict__ out_z) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int S = S_out;
   const long long per = n * n_rec * S;
@@ -77,7 +77,7 @@ __global__ void k_fetch_traces(const R* __restrict__ tr, int n_rec, int S_lay, i
   rem -= (long long)s * n * n_rec;
   const long long t = rem / n_rec;
   const int r = (int)(rem - t * n_rec);
-  out[q] = (double)tr[(((t0 + t) * 2 + comp) * n_rec + r) * (long long)S_lay + s];
+  (comp ? out_z : out_x)[q - comp * per] = (double)tr[(((t0 + t) * 2 + comp) * n_rec + r) * (long long)S_lay + s];
 }
 
 // 1/2 sum_e J_e sum_ij M_ij [rho v_i.v_j + compliance(sigma_i, sigma_j)], FP64 accumulation.

@@ -1456,24 +1456,38 @@ int dg_gpu_step_profiled(dg_gpu_ctx* c, long n, int flush_l2, float* ms_vel, flo
 }
 
 int dg_gpu_fetch_traces(dg_gpu_ctx* c, int mesh, long t0, long n, double* dst_x, double* dst_z) {
-  if (!c || !dst_x || !dst_z || mesh < 0 || mesh >= (int)c->mi.size() || t0 < 0 || n < 0)
+  if (!c || !dst_x || !dst_z || mesh < DG_ALL_MESHES || mesh >= (int)c->mi.size() || t0 < 0 || n < 0)
     return fail(DG_ERR_ARG, "bad arguments");
-  const MeshHostInfo& h = c->mi[mesh];
-  if (t0 + n > std::min(c->t, h.steps)) return fail(DG_ERR_STATE, "trace window beyond the steps taken");
-  const long long per = (long long)n * h.n_rec * h.S;
-  if (per == 0) return DG_OK;
+  // the meshes asked for, their blocks one after the other in both outputs
+  const int k0 = mesh == DG_ALL_MESHES ? 0 : mesh, k1 = mesh == DG_ALL_MESHES ? (int)c->mi.size() : mesh + 1;
+  long long total = 0;
+  for (int k = k0; k < k1; k++) {
+    const MeshHostInfo& h = c->mi[k];
+    if (t0 + n > std::min(c->t, h.steps)) return fail(DG_ERR_STATE, "trace window beyond the steps taken");
+    total += (long long)n * h.n_rec * h.S;
+  }
+  if (total == 0) return DG_OK;
   CK(cudaSetDevice(c->device));
-  int rc = ensure_stage(c, (size_t)2 * per);
+  int rc = ensure_stage(c, (size_t)2 * total);
   if (rc) return rc;
   const int B = 256;
-  const int grid = (int)((2 * per + B - 1) / B);
-  if (c->is_double)
-    k_fetch_traces<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].trace, h.n_rec, h.S_pad, h.S, t0, n, c->d_stage);
-  else
-    k_fetch_traces<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].trace, h.n_rec, h.S_pad, h.S, t0, n, c->d_stage);
-  CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(dst_x, c->d_stage, per * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(dst_z, c->d_stage + per, per * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  long long at = 0;
+  for (int k = k0; k < k1; k++) {
+    const MeshHostInfo& h = c->mi[k];
+    const long long per = (long long)n * h.n_rec * h.S;
+    if (per == 0) continue;
+    const int grid = (int)((2 * per + B - 1) / B);
+    double* ox = c->d_stage + at;
+    double* oz = c->d_stage + total + at;
+    if (c->is_double)
+      k_fetch_traces<double><<<grid, B, 0, c->stream>>>(c->md_d[k].trace, h.n_rec, h.S_pad, h.S, t0, n, ox, oz);
+    else
+      k_fetch_traces<float><<<grid, B, 0, c->stream>>>(c->md_f[k].trace, h.n_rec, h.S_pad, h.S, t0, n, ox, oz);
+    CK(cudaGetLastError());
+    at += per;
+  }
+  CK(cudaMemcpyAsync(dst_x, c->d_stage, total * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(dst_z, c->d_stage + total, total * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return DG_OK;
 }
@@ -1830,11 +1844,17 @@ int dg_gpu_debug_stall_wave(dg_gpu_ctx* c, int unit) {
 }
 
 int dg_gpu_set_wavelet(dg_gpu_ctx* c, int mesh, long t0, long n, const double* w) {
-  if (!c || !w || mesh < 0 || mesh >= (int)c->mi.size() || t0 < 0 || n < 0 || t0 + n > c->mi[mesh].steps)
+  if (!c || !w || mesh < DG_ALL_MESHES || mesh >= (int)c->mi.size() || t0 < 0 || n < 0)
     return fail(DG_ERR_ARG, "bad arguments");
+  const int k0 = mesh == DG_ALL_MESHES ? 0 : mesh, k1 = mesh == DG_ALL_MESHES ? (int)c->mi.size() : mesh + 1;
+  for (int k = k0; k < k1; k++)
+    if (t0 + n > c->mi[k].steps) return fail(DG_ERR_ARG, "wavelet window beyond a mesh's steps");
   CK(cudaSetDevice(c->device));
-  const double* dw = c->is_double ? c->md_d[mesh].wavelet : c->md_f[mesh].wavelet;
-  CK(cudaMemcpyAsync((void*)(dw + t0), w, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  for (int k = k0; k < k1; k++) {  // mesh k's samples follow those of the meshes before it
+    const double* dw = c->is_double ? c->md_d[k].wavelet : c->md_f[k].wavelet;
+    CK(cudaMemcpyAsync((void*)(dw + t0), w + (size_t)(k - k0) * n, n * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+  }
   CK(cudaStreamSynchronize(c->stream));
   return DG_OK;
 }

@@ -41,6 +41,8 @@ EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_tim
            "dg_gpu_context_stream"]
 # parts of a half step (dg_gpu_half_step_part)
 PART_ALL, PART_BOUNDARY, PART_INTERIOR = 0, 1, 2
+# every mesh of the context at once (dg_gpu_fetch_traces, dg_gpu_set_wavelet)
+ALL_MESHES = -1
 
 
 def energy_noalloc(device: int, K: int, fields, jacobi, A, inverV: np.ndarray, out, stream=None) -> None:
@@ -296,9 +298,13 @@ class Engine:
         _check(lib().dg_gpu_halo_unpack(self._ctx, mesh, int(what), C.c_void_p(dev_ptr)), "dg_gpu_halo_unpack")
 
     def fetch_traces(self, t0: int, n: int, mesh: int = 0, out_x=None, out_z=None):
-        """Traces of steps [t0, t0+n) of all shots, shape (shots, n, n_rec) each."""
-        inf = self.info[mesh]
-        shape = (inf["S"], int(n), inf["R"])
+        """Traces of steps [t0, t0+n) of all shots, shape (shots, n, n_rec) each; mesh =
+        ALL_MESHES: every mesh's block one after the other, flat (sum of shots * n * n_rec)."""
+        if mesh == ALL_MESHES:
+            shape = (sum(inf["S"] * inf["R"] for inf in self.info) * int(n),)
+        else:
+            inf = self.info[mesh]
+            shape = (inf["S"], int(n), inf["R"])
         ox = np.empty(shape) if out_x is None else out_x
         oz = np.empty(shape) if out_z is None else out_z
         _check(lib().dg_gpu_fetch_traces(self._ctx, mesh, int(t0), int(n), _ptr(ox), _ptr(oz)), "dg_gpu_fetch_traces")
@@ -335,9 +341,13 @@ class Engine:
         _check(lib().dg_gpu_reset(self._ctx), "dg_gpu_reset")
 
     def set_wavelet(self, t0: int, w, mesh: int = 0):
+        """Wavelet samples from step t0 on; mesh = ALL_MESHES: w holds the same number of samples
+        for each mesh, one mesh after the other."""
         if not hasattr(w, "data_ptr"):
             w = np.ascontiguousarray(w, dtype=np.float64)
         n = w.numel() if hasattr(w, "numel") else w.size
+        if mesh == ALL_MESHES:
+            n //= len(self.info)
         _check(lib().dg_gpu_set_wavelet(self._ctx, mesh, int(t0), n, _ptr(w)), "dg_gpu_set_wavelet")
 
     def flush_l2(self):

@@ -147,7 +147,10 @@ int dg_gpu_step_timed(dg_gpu_ctx *ctx, long n);
 int dg_gpu_step_profiled(dg_gpu_ctx *ctx, long n, int flush_l2, float *ms_vel, float *ms_str, double *ms_total);
 
 /* Receiver traces of steps [t0, t0+n) for every shot of one mesh:
- * dst_x / dst_z = double[n_shots][n][n_rec] (each shot like the reference's record_x window). */
+ * dst_x / dst_z = double[n_shots][n][n_rec] (each shot like the reference's record_x window).
+ * mesh = DG_ALL_MESHES: those blocks of every mesh one after the other, in mesh order, with one
+ * synchronisation. */
+#define DG_ALL_MESHES (-1)
 int dg_gpu_fetch_traces(dg_gpu_ctx *ctx, int mesh, long t0, long n, double *dst_x, double *dst_z);
 
 /* Copy one item of one mesh/shot to host memory `dst`, in the reference's layout:
@@ -162,7 +165,8 @@ int dg_gpu_load(dg_gpu_ctx *ctx, int what, int mesh, int shot, const double *src
 int dg_gpu_reset(dg_gpu_ctx *ctx);
 
 /* Replace wavelet samples [t0, t0+n) of one mesh with host values (the reference computes
- * w(t) on the host every step, DG_leap_Frog_OpenMP.c:421). */
+ * w(t) on the host every step, DG_leap_Frog_OpenMP.c:421); mesh = DG_ALL_MESHES: w holds n
+ * samples for each mesh, one after the other in mesh order. */
 int dg_gpu_set_wavelet(dg_gpu_ctx *ctx, int mesh, long t0, long n, const double *w);
 
 /* ---- one mesh split over several contexts (one per GPU): domain decomposition --------------

@@ -94,3 +94,26 @@ def test_persistent_batch_barrier_limit_reports_timeout(meshes, monkeypatch):
         fields = [e.fetch(f, k, m) for k, (_, _, S) in enumerate(SPEC) for m in range(S) for f in FIELDS]
     for x, y in zip(ref[1], fields):
         assert np.array_equal(x, y)
+
+
+def test_all_meshes_trace_fetch_and_wavelet(meshes):
+    """DG_ALL_MESHES: one call fetches every mesh's traces (blocks in mesh order) and one call
+    sets every mesh's wavelet samples; both equal the per-mesh calls."""
+    rng = np.random.default_rng(4)
+    n = 80
+    new = rng.normal(size=(len(SPEC), n))
+    out = []
+    for together in (False, True):
+        with eng.Engine(meshes, "fp32") as e:
+            if together:
+                e.set_wavelet(0, new.ravel(), mesh=eng.ALL_MESHES)
+            else:
+                for k in range(len(SPEC)):
+                    e.set_wavelet(0, new[k], mesh=k)
+            e.step(120)
+            per = [e.fetch_traces(0, n, mesh=k) for k in range(len(SPEC))]
+            ax, az = e.fetch_traces(0, n, mesh=eng.ALL_MESHES)
+            assert np.array_equal(ax, np.concatenate([p[0].ravel() for p in per]))
+            assert np.array_equal(az, np.concatenate([p[1].ravel() for p in per]))
+            out.append(az)
+    assert np.array_equal(out[0], out[1]) and np.abs(out[0]).max() > 0

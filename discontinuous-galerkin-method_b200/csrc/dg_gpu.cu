@@ -1379,7 +1379,7 @@ static int enqueue_steps(dg_gpu_ctx* c, long n, bool timed) {
   return DG_OK;
 }
 
-static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
+static int do_steps(dg_gpu_ctx* c, long n, bool timed, bool wait = true) {
   if (!c || n < 0) return fail(DG_ERR_ARG, "bad arguments");
   if (c->half_pending || c->part_done)
     return fail(DG_ERR_STATE, "a half step is waiting for its other half or part");
@@ -1387,12 +1387,20 @@ static int do_steps(dg_gpu_ctx* c, long n, bool timed) {
   CK(cudaSetDevice(c->device));
   int rc = enqueue_steps(c, n, timed);
   if (rc) return rc;
-  CK(cudaStreamSynchronize(c->stream));
   c->stats.steps_done = c->t;
+  if (!wait) return DG_OK;
+  CK(cudaStreamSynchronize(c->stream));
   return check_wave(c);
 }
 
 int dg_gpu_step(dg_gpu_ctx* c, long n) { return do_steps(c, n, false); }
+int dg_gpu_step_async(dg_gpu_ctx* c, long n) { return do_steps(c, n, false, false); }
+int dg_gpu_synchronize(dg_gpu_ctx* c) {
+  if (!c) return fail(DG_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  return check_wave(c);
+}
 int dg_gpu_step_timed(dg_gpu_ctx* c, long n) { return do_steps(c, n, true); }
 
 static int ensure_flush(dg_gpu_ctx* c) {

@@ -32,7 +32,7 @@ def _ptr(a):
     return a.ctypes.data
 
 
-EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_timed", "dg_gpu_step_profiled",
+EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_async", "dg_gpu_synchronize", "dg_gpu_step_timed", "dg_gpu_step_profiled",
            "dg_gpu_fetch_traces", "dg_gpu_fetch", "dg_gpu_load",
            "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_steps_done",
            "dg_gpu_free", "dg_gpu_strerror", "dg_gpu_last_error", "dg_gpu_energy_noalloc",
@@ -115,6 +115,8 @@ def lib(path: str | None = None):
         L.dg_gpu_default_opts.argtypes = [C.c_void_p]
         L.dg_gpu_init.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         L.dg_gpu_step.argtypes = [C.c_void_p, C.c_long]
+        L.dg_gpu_step_async.argtypes = [C.c_void_p, C.c_long]
+        L.dg_gpu_synchronize.argtypes = [C.c_void_p]
         L.dg_gpu_step_timed.argtypes = [C.c_void_p, C.c_long]
         L.dg_gpu_step_profiled.argtypes = [C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.dg_gpu_step_profiled.restype = C.c_int
@@ -149,8 +151,9 @@ def lib(path: str | None = None):
         L.dg_gpu_strerror.restype = C.c_char_p
         L.dg_gpu_strerror.argtypes = [C.c_int]
         L.dg_gpu_last_error.restype = C.c_char_p
-        for n in ("dg_gpu_init", "dg_gpu_step", "dg_gpu_step_timed", "dg_gpu_fetch", "dg_gpu_load", "dg_gpu_reset",
-                  "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_free"):
+        for n in ("dg_gpu_init", "dg_gpu_step", "dg_gpu_step_async", "dg_gpu_synchronize", "dg_gpu_step_timed",
+                  "dg_gpu_fetch", "dg_gpu_load", "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2",
+                  "dg_gpu_stats_get", "dg_gpu_free"):
             getattr(L, n).restype = C.c_int
         _LIB = L
     return _LIB
@@ -238,6 +241,13 @@ class Engine:
     # -- the reference's loop body ---------------------------------------------------------
     def step(self, n: int = 1):
         _check(lib().dg_gpu_step(self._ctx, int(n)), "dg_gpu_step")
+
+    def step_async(self, n: int = 1):
+        """Enqueue n steps and return; `synchronize` waits for them (fetches wait by themselves)."""
+        _check(lib().dg_gpu_step_async(self._ctx, int(n)), "dg_gpu_step_async")
+
+    def synchronize(self):
+        _check(lib().dg_gpu_synchronize(self._ctx), "dg_gpu_synchronize")
 
     def step_timed(self, n: int = 1):
         _check(lib().dg_gpu_step_timed(self._ctx, int(n)), "dg_gpu_step_timed")

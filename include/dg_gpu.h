@@ -134,6 +134,13 @@ int dg_gpu_init(dg_gpu_ctx **ctx, const dg_gpu_mesh *meshes, int n_meshes, const
  * Stepping past the longest wavelet table returns DG_ERR_STATE without doing anything. */
 int dg_gpu_step(dg_gpu_ctx *ctx, long n);
 
+/* The same steps, enqueued on the context stream without waiting for them (with the NaN
+ * watchdog on, its checks still wait): the host is free until dg_gpu_synchronize, which waits
+ * and reports a wait limit reached on the way (DG_ERR_TIMEOUT).  Every other call of the context
+ * is ordered after the enqueued steps (fetches wait for them). */
+int dg_gpu_step_async(dg_gpu_ctx *ctx, long n);
+int dg_gpu_synchronize(dg_gpu_ctx *ctx);
+
 /* Same, timing each velocity and stress half-step with CUDA events on the context stream;
  * the sums land in dg_gpu_stats (ms_velocity, ms_stress). */
 int dg_gpu_step_timed(dg_gpu_ctx *ctx, long n);

@@ -117,3 +117,23 @@ def test_all_meshes_trace_fetch_and_wavelet(meshes):
             assert np.array_equal(az, np.concatenate([p[1].ravel() for p in per]))
             out.append(az)
     assert np.array_equal(out[0], out[1]) and np.abs(out[0]).max() > 0
+
+
+@pytest.mark.parametrize("precision,wave", [("fp32", -1), ("fp32", 0), ("fp64", -1)])
+def test_async_steps_equal_synchronous_steps(meshes, precision, wave):
+    """dg_gpu_step_async + dg_gpu_synchronize give the steps of dg_gpu_step; fetches after
+    enqueued steps wait for them by themselves."""
+    out = []
+    for use_async in (False, True):
+        with eng.Engine(meshes[3], precision, wavefront=wave) as e:   # 16 shots: wavefront when on
+            if use_async:
+                e.step_async(40)
+                e.step_async(60)
+                e.synchronize()
+                e.step_async(50)
+            else:
+                e.step(150)
+            out.append([e.fetch("Vz", 0, s) for s in (0, 15)] + [e.fetch("trace_z", 0, 15)])
+            assert e.steps_done == 150
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)

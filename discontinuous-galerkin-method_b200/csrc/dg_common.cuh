@@ -112,6 +112,16 @@ template <class R> struct MeshDev {
 // kernel writes only the counter the other one reads, so a captured graph can be replayed.
 struct Counters { long long v, s; };
 
+// Programmatic dependent launch (two-launch step kernels): wait until the previous kernel of the
+// stream has completed and its stores are visible — at once when this launch did not ask to
+// start early — then let the next kernel of the stream start its blocks, which wait the same way.
+// The next kernel starts only once every block of this one has started, so no block waits for
+// room that a waiting block holds.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // gpu-scope acquire load / release store of a flag, and a volatile load of an error word
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   unsigned v;

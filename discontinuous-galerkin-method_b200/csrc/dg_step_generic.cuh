@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(256, 2) k_velocity(const __grid_constant__ Ops
                                                      const MeshDev<R>* __restrict__ tab,
                                                      const int2* __restrict__ btab,
                                                      Counters* __restrict__ ctr) {
+  pdl_enter();
   int lb;
   const MeshDev<R>& m = *pick_mesh<MULTI>(one, tab, btab, lb);
   const long long t = ctr->v;
@@ -393,6 +394,7 @@ __global__ void __launch_bounds__(256, 2) k_stress(const __grid_constant__ Ops<R
                                                    const MeshDev<R>* __restrict__ tab,
                                                    const int2* __restrict__ btab,
                                                    Counters* __restrict__ ctr) {
+  pdl_enter();
   int lb;
   const MeshDev<R>& m = *pick_mesh<MULTI>(one, tab, btab, lb);
   const long long t = ctr->s;

@@ -93,6 +93,7 @@ __global__ void __launch_bounds__(256, 2) k_velocity_mx(const __grid_constant__ 
                                                         const MeshDev<float>* __restrict__ tab,
                                                         const int2* __restrict__ btab,
                                                         Counters* __restrict__ ctr) {
+  pdl_enter();
   const int2 b = __ldg(btab + blockIdx.x);
   const long long t = ctr->v;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
@@ -105,6 +106,7 @@ __global__ void __launch_bounds__(256, 2) k_stress_mx(const __grid_constant__ Op
                                                       const MeshDev<float>* __restrict__ tab,
                                                       const int2* __restrict__ btab,
                                                       Counters* __restrict__ ctr) {
+  pdl_enter();
   const int2 b = __ldg(btab + blockIdx.x);
   const long long t = ctr->s;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;

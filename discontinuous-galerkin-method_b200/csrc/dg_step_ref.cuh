@@ -19,6 +19,7 @@ __global__ void __launch_bounds__(256) k_velocity_ref(const __grid_constant__ Op
                                                       const MeshDev<double>* __restrict__ tab,
                                                       const int2* __restrict__ btab,
                                                       Counters* __restrict__ ctr) {
+  pdl_enter();
   int lb;
   const MeshDev<double>& m = *pick_mesh<MULTI>(one, tab, btab, lb);
   const long long t = ctr->v;
@@ -126,6 +127,7 @@ __global__ void __launch_bounds__(256) k_stress_ref(const __grid_constant__ Ops<
                                                     const MeshDev<double>* __restrict__ tab,
                                                     const int2* __restrict__ btab,
                                                     Counters* __restrict__ ctr) {
+  pdl_enter();
   int lb;
   const MeshDev<double>& m = *pick_mesh<MULTI>(one, tab, btab, lb);
   const long long t = ctr->s;

@@ -207,6 +207,7 @@ template <int S, bool KAHAN, bool PM = false>
 __global__ void __launch_bounds__(256, 2) k_velocity_x2(const __grid_constant__ Ops2 ops,
                                                         const __grid_constant__ MeshDev<float> m,
                                                         Counters* __restrict__ ctr) {
+  pdl_enter();
   const long long t = ctr->v;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
   if (t >= m.steps) return;
@@ -370,6 +371,7 @@ template <int S, bool KAHAN, bool PM = false>
 __global__ void __launch_bounds__(256, 2) k_stress_x2(const __grid_constant__ Ops2 ops,
                                                       const __grid_constant__ MeshDev<float> m,
                                                       Counters* __restrict__ ctr) {
+  pdl_enter();
   const long long t = ctr->s;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
   if (t >= m.steps) return;
@@ -547,6 +549,7 @@ template <bool KAHAN>
 __global__ void __launch_bounds__(256, 2) k_velocity_x2e(const __grid_constant__ Ops2 ops,
                                                          const __grid_constant__ MeshDev<float> m,
                                                          Counters* __restrict__ ctr) {
+  pdl_enter();
   const long long t = ctr->v;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
   if (t >= m.steps) return;
@@ -663,6 +666,7 @@ template <bool KAHAN>
 __global__ void __launch_bounds__(256, 2) k_stress_x2e(const __grid_constant__ Ops2 ops,
                                                        const __grid_constant__ MeshDev<float> m,
                                                        Counters* __restrict__ ctr) {
+  pdl_enter();
   const long long t = ctr->s;
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->v = t + 1;
   if (t >= m.steps) return;

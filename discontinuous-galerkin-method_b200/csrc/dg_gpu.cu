@@ -161,6 +161,9 @@ struct dg_gpu_ctx {
   bool multi = false;
   int graph_steps = 100;
   cudaGraphExec_t graph = nullptr;
+  // a second graph of graph_steps / 4 steps, for calls of fewer steps than a whole graph
+  cudaGraphExec_t graph_small = nullptr;
+  int graph_small_steps = 0;
   int graph_block = 0;
   long t = 0;
   long max_steps = 0;
@@ -177,6 +180,7 @@ struct dg_gpu_ctx {
 
   ~dg_gpu_ctx() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (graph_small) cudaGraphExecDestroy(graph_small);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     for (int k = 0; k < 2; k++) {
@@ -1004,22 +1008,38 @@ int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid =
   return DG_OK;
 }
 
-int rebuild_graph(dg_gpu_ctx* c) {
-  if (c->graph) {
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-  }
-  if (c->graph_steps <= 0 || c->mx_persistent) return DG_OK;  // the persistent batch loops on the device
+// Capture `steps` steps into an instantiated graph, uploaded now so the first launch does not
+// pay for it.
+static int capture_steps(dg_gpu_ctx* c, int steps, cudaGraphExec_t* out) {
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   int rc = DG_OK;
-  for (int k = 0; k < c->graph_steps && rc == DG_OK; k++) rc = launch_step(c);
+  for (int k = 0; k < steps && rc == DG_OK; k++) rc = launch_step(c);
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (rc) return rc;
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __LINE__);
-  e = cudaGraphInstantiate(&c->graph, g, 0);
+  e = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __LINE__);
+  CK(cudaGraphUpload(*out, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DG_OK;
+}
+
+int rebuild_graph(dg_gpu_ctx* c) {
+  for (cudaGraphExec_t* gp : {&c->graph, &c->graph_small})
+    if (*gp) {
+      cudaGraphExecDestroy(*gp);
+      *gp = nullptr;
+    }
+  c->graph_small_steps = 0;
+  if (c->graph_steps <= 0 || c->mx_persistent) return DG_OK;  // the persistent batch loops on the device
+  int rc = capture_steps(c, c->graph_steps, &c->graph);
+  if (rc) return rc;
+  if (c->graph_steps >= 8) {
+    c->graph_small_steps = c->graph_steps / 4;
+    if ((rc = capture_steps(c, c->graph_small_steps, &c->graph_small))) return rc;
+  }
   c->graph_block = c->block;
   return DG_OK;
 }
@@ -1383,6 +1403,9 @@ static int enqueue_steps(dg_gpu_ctx* c, long n, bool timed) {
       long k = 0;
       if (c->graph && c->graph_steps > 0)
         for (; k + c->graph_steps <= chunk; k += c->graph_steps) CK(cudaGraphLaunch(c->graph, c->stream));
+      if (c->graph_small && c->graph_small_steps > 0)
+        for (; k + c->graph_small_steps <= chunk; k += c->graph_small_steps)
+          CK(cudaGraphLaunch(c->graph_small, c->stream));
       for (; k < chunk; k++) {
         int rc = launch_step(c);
         if (rc) return rc;

@@ -92,7 +92,8 @@ typedef struct {
 	int device;          /* CUDA device ordinal */
 	int reorder;         /* 1: renumber elements along a Hilbert curve of centroids for locality */
 	int block_threads;   /* threads per block, 0: automatic (or autotuned) */
-	int graph_steps;     /* steps per captured CUDA graph, 0: automatic, <0: no graphs */
+	int graph_steps;     /* steps per captured CUDA graph (plus one of a quarter of them for shorter
+	                        calls), 0: automatic (100), <0: no graphs */
 	int autotune;        /* 1: time candidate block sizes (and, for a batch of meshes, the persistent or
 	                        two-launch step; for the wavefront step its persistent form and lag) at init */
 	int watchdog_every;  /* check the velocity fields for NaN/Inf every k steps (0: off) */

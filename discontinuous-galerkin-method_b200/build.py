@@ -25,7 +25,7 @@ GPU_DEPS = GPU_SRC + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endsw
     [os.path.join(INCLUDE, "dg_gpu.h")]
 
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-              "-Xcompiler", "-fPIC,-fopenmp", "-shared", "--expt-relaxed-constexpr", "-Xptxas", "-v", "-lgomp"]
+              "-Xcompiler", "-fPIC,-fopenmp,-ffp-contract=off", "-shared", "--expt-relaxed-constexpr", "-Xptxas", "-v", "-lgomp"]
 
 
 def _stale(target, deps):

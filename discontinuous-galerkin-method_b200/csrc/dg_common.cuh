@@ -74,6 +74,10 @@ template <class R> struct Ops {
   R Ds[NP * NP];
   R L[NF * NP * NF];
   R M[NP * NP];  // reference mass matrix inv(V V^T), energy only
+  // the parsed Vr, Vs, inv(V): the reference-operator path rebuilds Dx, Dz from them
+  R Vr[NP * NP];
+  R Vs[NP * NP];
+  R Vi[NP * NP];
 };
 
 template <class R> struct MeshDev {

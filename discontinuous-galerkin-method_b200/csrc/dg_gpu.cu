@@ -128,6 +128,8 @@ struct dg_gpu_ctx {
   // before it in `pdl_enter`: measured -1.6 % (388k one-shot mesh) to +1.6 % (200k, two shots),
   // so off unless DG_PDL=1
   bool pdl = false;
+  // reference-operator path: Dx, Dz rebuilt in the kernels (one mesh, one shot, checked at set-up)
+  bool ref_otf = false;
   unsigned mx_extra = 0, mx_spin = 1u << 22;  // barrier arrivals beyond the grid, poll limit
   unsigned* d_mxbar = nullptr;
   int* d_mxerr = nullptr;
@@ -239,6 +241,7 @@ struct Prepared {
   std::vector<double> src_fun;  // [S][6]
   std::vector<int> rec_elem, rec_node;
   std::vector<double> Dx, Dz, Q, AB;  // SoA, reference path only
+  bool ref_otf = false;  // reference path: Dx, Dz rebuilt in the kernels (then not stored)
   long sponge_elems = 0;
 };
 
@@ -325,7 +328,7 @@ std::vector<int> rcm_order(const dg_gpu_mesh& m, long K) {
   return seq;
 }
 
-int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
+int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p, bool want_otf = false) {
   if (m.K <= 0 || m.K > (1L << 26)) return fail(DG_ERR_ARG, "K must be in [1, 2^26]");
   if (m.Np != 6 || m.Nfp != 3) return fail(DG_ERR_UNSUPPORTED, "only P2 (Np = 6, Nfp = 3) is supported");
   if (!m.Point || !m.Triangle || m.n_points <= 0 || !m.Vr || !m.Vs || !m.inverV || !m.S || !m.ibe || !m.Neighbor ||
@@ -487,17 +490,53 @@ int prepare(const dg_gpu_mesh& m, int precision, int reorder, Prepared& p) {
     p.rec_node[r] = (int)node;
   }
   if (precision == DG_FP64_REF) {
-    p.Dx.assign((size_t)36 * Kp, 0.0);
-    p.Dz.assign((size_t)36 * Kp, 0.0);
+    // Dx, Dz rebuilt in the kernels when, for every element, the operations of Dx_Dz
+    // (fun_DG.c:1166-1190: dxd = Rx Vr + Sx Vs, then dxd inv(V), each product and sum rounded on
+    // its own, as here) give exactly the caller's arrays from this element's Rx, Sx, Rz, Sz
+    bool otf = want_otf;
+    if (otf) {
+      int differ = 0;
+#pragma omp parallel for schedule(static) reduction(| : differ)
+      for (long e = 0; e < K; e++) {
+        if (differ) continue;
+        const double* g = &rxa[e * 4];  // Rx, Sx, Rz, Sz
+        for (int i = 0; i < 6 && !differ; i++) {
+          double ax[6], az[6];
+          for (int k = 0; k < 6; k++) {
+            const double a1 = g[0] * m.Vr[i * 6 + k], a2 = g[1] * m.Vs[i * 6 + k];
+            const double b1 = g[2] * m.Vr[i * 6 + k], b2 = g[3] * m.Vs[i * 6 + k];
+            ax[k] = a1 + a2;
+            az[k] = b1 + b2;
+          }
+          for (int q = 0; q < 6; q++) {
+            double fx = 0, fz = 0;
+            for (int k = 0; k < 6; k++) {
+              const double px = ax[k] * m.inverV[k * 6 + q], pz = az[k] * m.inverV[k * 6 + q];
+              fx = fx + px;
+              fz = fz + pz;
+            }
+            differ |= memcmp(&fx, &m.Dx[e * 36 + i * 6 + q], sizeof(double)) != 0 ||
+                      memcmp(&fz, &m.Dz[e * 36 + i * 6 + q], sizeof(double)) != 0;
+          }
+        }
+      }
+      otf = !differ;
+    }
+    p.ref_otf = otf;
+    if (!otf) {
+      p.Dx.assign((size_t)36 * Kp, 0.0);
+      p.Dz.assign((size_t)36 * Kp, 0.0);
+    }
     p.Q.assign((size_t)30 * Kp, 0.0);
     p.AB.assign((size_t)10 * Kp, 0.0);
 #pragma omp parallel for schedule(static)
     for (long n = 0; n < K; n++) {
       const long e = p.order[n];
-      for (int q = 0; q < 36; q++) {
-        p.Dx[(size_t)q * Kp + n] = m.Dx[e * 36 + q];
-        p.Dz[(size_t)q * Kp + n] = m.Dz[e * 36 + q];
-      }
+      if (!otf)
+        for (int q = 0; q < 36; q++) {
+          p.Dx[(size_t)q * Kp + n] = m.Dx[e * 36 + q];
+          p.Dz[(size_t)q * Kp + n] = m.Dz[e * 36 + q];
+        }
       for (int q = 0; q < 30; q++) p.Q[(size_t)q * Kp + n] = m.Q[e * 30 + q];
       for (int q = 0; q < 5; q++) {
         p.AB[(size_t)q * Kp + n] = m.A[e * 5 + q];
@@ -574,8 +613,9 @@ int upload_mesh(dg_gpu_ctx* c, const dg_gpu_mesh& m, Prepared& p, MeshDev<R>& d)
   CK(cudaMemsetAsync(d.trace, 0, sizeof(R) * trace_elems, c->stream));
   if (c->precision == DG_FP64_REF) {
     double *dx, *dz, *q, *ab;
-    if ((rc = c->upload(&dx, p.Dx))) return rc;
-    if ((rc = c->upload(&dz, p.Dz))) return rc;
+    dx = dz = nullptr;  // absent when the kernels rebuild them
+    if (!p.Dx.empty() && (rc = c->upload(&dx, p.Dx))) return rc;
+    if (!p.Dz.empty() && (rc = c->upload(&dz, p.Dz))) return rc;
     if ((rc = c->upload(&q, p.Q))) return rc;
     if ((rc = c->upload(&ab, p.AB))) return rc;
     d.Dx = dx;
@@ -620,6 +660,11 @@ template <class R> void fill_ops(Ops<R>& o, const dg_gpu_mesh& m) {
       o.Ds[i * 6 + q] = (R)b;
     }
   for (int q = 0; q < 54; q++) o.L[q] = (R)m.S[q];
+  for (int q = 0; q < 36; q++) {
+    o.Vr[q] = (R)m.Vr[q];
+    o.Vs[q] = (R)m.Vs[q];
+    o.Vi[q] = (R)m.inverV[q];
+  }
   // reference mass matrix inv(V V^T) = inverV^T inverV
   for (int i = 0; i < 6; i++)
     for (int k = 0; k < 6; k++) {
@@ -943,13 +988,21 @@ int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid =
   if (before_t) CK(cudaEventRecord(before_t, st));
   if (c->precision == DG_FP64_REF) {
     if (c->multi) {
-      if (hv) DG_LAUNCH((k_velocity_ref<true>), gv, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
+      if (hv) DG_LAUNCH((k_velocity_ref<true, false>), gv, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
       if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress_ref<true>), gt, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
+      if (ht) DG_LAUNCH((k_stress_ref<true, false>), gt, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
     } else {
-      if (hv) DG_LAUNCH((k_velocity_ref<false>), gv, c->ops_d, c->md_d[0], (const MeshDev<double>*)nullptr, (const int2*)nullptr, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress_ref<false>), gt, c->ops_d, c->md_d[0], (const MeshDev<double>*)nullptr, (const int2*)nullptr, c->d_ctr);
+      const MeshDev<double>* no_tab = nullptr;
+      const int2* no_btab = nullptr;
+      if (c->ref_otf) {
+        if (hv) DG_LAUNCH((k_velocity_ref<false, true>), gv, c->ops_d, c->md_d[0], no_tab, no_btab, c->d_ctr);
+        if (mid) CK(cudaEventRecord(mid, st));
+        if (ht) DG_LAUNCH((k_stress_ref<false, true>), gt, c->ops_d, c->md_d[0], no_tab, no_btab, c->d_ctr);
+      } else {
+        if (hv) DG_LAUNCH((k_velocity_ref<false, false>), gv, c->ops_d, c->md_d[0], no_tab, no_btab, c->d_ctr);
+        if (mid) CK(cudaEventRecord(mid, st));
+        if (ht) DG_LAUNCH((k_stress_ref<false, false>), gt, c->ops_d, c->md_d[0], no_tab, no_btab, c->d_ctr);
+      }
     }
   } else if (c->is_double) {
     if (c->multi) {
@@ -1275,7 +1328,14 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
                (p.kind == 1 && o.wavefront == 1));
     if (o.wavefront == 1 && !c->wave)
       return fail(DG_ERR_UNSUPPORTED, "the wavefront step needs one FP32 mesh with 1, 2, 4, 8, ..., 128 shots");
-    int rc = prepare(meshes[k], o.precision, c->wave ? 2 : o.reorder, p);
+    const char* arrays = getenv("DG_REF_ARRAYS");
+    // rebuilt Dx, Dz for one large one-shot mesh: 200k elements 56.1 against 52.6 G DOF-updates/s,
+    // 388k 58.6 against 56.6, and 576 bytes per element less device memory; on 20k elements the
+    // register-heavy rebuild is slower (37.3 against 48.8), so small meshes keep the arrays
+    const bool want_otf = o.precision == DG_FP64_REF && n_meshes == 1 && meshes[k].n_shots == 1 &&
+                          meshes[k].K >= 65536 && !(arrays && atoi(arrays) != 0);
+    int rc = prepare(meshes[k], o.precision, c->wave ? 2 : o.reorder, p, want_otf);
+    if (n_meshes == 1) c->ref_otf = p.ref_otf;
     if (rc) return rc;
     MeshHostInfo& h = c->mi[k];
     h.K = p.K;

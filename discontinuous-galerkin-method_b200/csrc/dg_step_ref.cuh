@@ -13,7 +13,43 @@ __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, 
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
 
-template <bool MULTI>
+// Row i of the element's Dx and Dz.  OTF: rebuilt from the element's (Rx, Sx, Rz, Sz) with the
+// operations of Dx_Dz (fun_DG.c:1166-1190), each product and sum rounded on its own:
+// dxd[i][k] = Rx Vr[i][k] + Sx Vs[i][k], then Dx[i][n] = sum over k = 0..5 of dxd[i][k] inv(V)[k][n]
+// from 0 — the same doubles the reference stores (the host checks that at set-up).  Otherwise
+// read from the caller's arrays.
+template <bool OTF>
+__device__ __forceinline__ void ref_rows(const Ops<double>& ops, const MeshDev<double>& m, int e, int i,
+                                         double (&dx)[NP], double (&dz)[NP]) {
+  if (OTF) {
+    const double4 g = ld4(m.geo + e);  // Rx, Sx, Rz, Sz
+    double ax[NP], az[NP];
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      ax[k] = add(mul(g.x, ops.Vr[i * NP + k]), mul(g.y, ops.Vs[i * NP + k]));
+      az[k] = add(mul(g.z, ops.Vr[i * NP + k]), mul(g.w, ops.Vs[i * NP + k]));
+    }
+#pragma unroll
+    for (int n = 0; n < NP; n++) {
+      double fx = 0, fz = 0;
+#pragma unroll
+      for (int k = 0; k < NP; k++) {
+        fx = add(fx, mul(ax[k], ops.Vi[k * NP + n]));
+        fz = add(fz, mul(az[k], ops.Vi[k * NP + n]));
+      }
+      dx[n] = fx;
+      dz[n] = fz;
+    }
+  } else {
+#pragma unroll
+    for (int n = 0; n < NP; n++) {
+      dx[n] = __ldg(m.Dx + (i * NP + n) * (long long)m.Kp + e);
+      dz[n] = __ldg(m.Dz + (i * NP + n) * (long long)m.Kp + e);
+    }
+  }
+}
+
+template <bool MULTI, bool OTF>
 __global__ void __launch_bounds__(256) k_velocity_ref(const __grid_constant__ Ops<double> ops,
                                                       const __grid_constant__ MeshDev<double> one,
                                                       const MeshDev<double>* __restrict__ tab,
@@ -59,10 +95,12 @@ __global__ void __launch_bounds__(256) k_velocity_ref(const __grid_constant__ Op
 #pragma unroll
   for (int i = 0; i < NP; i++) {
     double s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+    double dxr[NP], dzr[NP];
+    ref_rows<OTF>(ops, m, e, i, dxr, dzr);
 #pragma unroll
     for (int n = 0; n < NP; n++) {
-      const double dx = __ldg(m.Dx + (i * NP + n) * (long long)Kp + e);
-      const double dz = __ldg(m.Dz + (i * NP + n) * (long long)Kp + e);
+      const double dx = dxr[n];
+      const double dz = dzr[n];
       s1 = add(s1, mul(dx, txx[n]));
       s2 = add(s2, mul(dx, txz[n]));
       s3 = add(s3, mul(dz, tzz[n]));
@@ -121,7 +159,7 @@ __global__ void __launch_bounds__(256) k_velocity_ref(const __grid_constant__ Op
   }
 }
 
-template <bool MULTI>
+template <bool MULTI, bool OTF>
 __global__ void __launch_bounds__(256) k_stress_ref(const __grid_constant__ Ops<double> ops,
                                                     const __grid_constant__ MeshDev<double> one,
                                                     const MeshDev<double>* __restrict__ tab,
@@ -163,10 +201,12 @@ __global__ void __launch_bounds__(256) k_stress_ref(const __grid_constant__ Ops<
 #pragma unroll
   for (int i = 0; i < NP; i++) {
     double s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+    double dxr[NP], dzr[NP];
+    ref_rows<OTF>(ops, m, e, i, dxr, dzr);
 #pragma unroll
     for (int n = 0; n < NP; n++) {
-      const double dx = __ldg(m.Dx + (i * NP + n) * (long long)Kp + e);
-      const double dz = __ldg(m.Dz + (i * NP + n) * (long long)Kp + e);
+      const double dx = dxr[n];
+      const double dz = dzr[n];
       s1 = add(s1, mul(dx, vx[n]));
       s2 = add(s2, mul(dx, vz[n]));
       s3 = add(s3, mul(dz, vx[n]));

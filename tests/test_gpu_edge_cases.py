@@ -79,3 +79,27 @@ def test_mesh_without_receivers(precision, shots):
     for a, b in zip(*fields):
         assert np.array_equal(a, b)
     assert np.abs(fields[0][1]).max() > 0
+
+
+def test_reference_path_rebuilt_operators_equal_arrays_and_oracle(monkeypatch):
+    """DG_FP64_REF on one one-shot mesh of 65,536 elements or more rebuilds Dx, Dz in the
+    kernels (after checking on the host that they equal the caller's arrays): traces and fields
+    equal the array path and the CPU oracle bit for bit."""
+    import os
+    steps = 120
+    w = pkg.workloads.homogeneous_square(n_cells=182, steps=steps, n_rec=183)
+    s = pkg.host.build_setup(w)
+    assert s.K >= 65536
+    o = oracle.Oracle.from_setup(s)
+    o.reset()
+    rx, rz = o.run(0, steps, threads=os.cpu_count() or 1)
+    out = []
+    for arrays in ("1", "0"):
+        monkeypatch.setenv("DG_REF_ARRAYS", arrays)
+        with eng.Engine(eng.mesh_from_setup(s), "fp64_ref") as e:
+            e.step(steps)
+            out.append((e.fetch("trace_x"), e.fetch("trace_z"), e.fetch("Vz")))
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+    assert np.array_equal(out[1][0], rx) and np.array_equal(out[1][1], rz)
+    assert np.abs(rz).max() > 0

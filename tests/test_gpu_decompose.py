@@ -123,3 +123,22 @@ def test_half_step_parts_state(meshes):
         with pytest.raises(eng.DGError) as ei:
             e.half_step_part(0, 3)
         assert ei.value.code == -1
+
+
+@pytest.mark.parametrize("overlap", [True, False])
+def test_split_reference_path_with_rebuilt_operators(overlap):
+    """Parts of 65,536 elements or more take the reference path with Dx, Dz rebuilt in the
+    kernels; in half-step windows too they equal the undivided run bit for bit."""
+    w = pkg.workloads.homogeneous_square(n_cells=265, steps=60, n_rec=266)
+    s = pkg.host.build_setup(w, full=True)
+    mesh = eng.mesh_from_setup(s)
+    with eng.Engine(mesh, "fp64_ref", wavefront=-1) as whole:
+        whole.step(50)
+        want = [whole.fetch(f).reshape(-1, 6) for f in ("Vz", "Txx")] + [whole.fetch("trace_z")]
+    with dec.SplitRun(mesh, 2, "fp64_ref", overlap=overlap) as run:
+        assert min(p.own.size for p in run.parts) >= 65536
+        run.step(50)
+        got = [run.fetch(f) for f in ("Vz", "Txx")] + [run.traces("trace_z")]
+    for a, b in zip(want, got):
+        assert np.array_equal(a, b)
+    assert np.abs(want[0]).max() > 0    # the field (the wave reaches no receiver in 50 steps)

@@ -1527,6 +1527,9 @@ static int ensure_flush(dg_gpu_ctx* c) {
 
 static int ensure_stage(dg_gpu_ctx* c, size_t elems) {
   if (elems <= c->stage_elems) return DG_OK;
+  c->release(c->d_stage);  // the smaller one (after the stream has finished with it)
+  c->d_stage = nullptr;
+  c->stage_elems = 0;
   double* p = nullptr;
   int rc = c->alloc(&p, elems);
   if (rc) return rc;
@@ -1692,20 +1695,28 @@ int dg_gpu_step_snapshots(dg_gpu_ctx* c, long n, long every, int mesh, int shot,
 int dg_gpu_fetch(dg_gpu_ctx* c, int what, int mesh, int shot, double* dst) {
   if (!c || !dst || mesh < 0 || mesh >= (int)c->mi.size()) return fail(DG_ERR_ARG, "bad arguments");
   const MeshHostInfo& h = c->mi[mesh];
-  if (shot < 0 || shot >= h.S) return fail(DG_ERR_ARG, "shot out of range");
+  const bool all = shot == DG_ALL_SHOTS && what >= DG_VX && what <= DG_TXZ;
+  if (!all && (shot < 0 || shot >= h.S)) return fail(DG_ERR_ARG, "shot out of range");
   CK(cudaSetDevice(c->device));
   const int B = 256;
   if (what >= DG_VX && what <= DG_TXZ) {
+    // one shot, or every shot one after the other ([S][K][Np]) with one copy and one wait
     const long long n = h.K * 6;
+    const int s0 = all ? 0 : shot, s1 = all ? h.S : shot + 1;
+    int rc = ensure_stage(c, (size_t)n * (s1 - s0));
+    if (rc) return rc;
     const int grid = (int)((n + B - 1) / B);
-    if (c->is_double)
-      k_fetch_field<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].U, what * 6, c->md_d[mesh].ES, c->md_d[mesh].PS, shot,
-                                                       h.d_new_of_old, (int)h.K, c->d_stage);
-    else
-      k_fetch_field<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].U, what * 6, c->md_f[mesh].ES, c->md_f[mesh].PS, shot,
-                                                      h.d_new_of_old, (int)h.K, c->d_stage);
+    for (int s = s0; s < s1; s++) {
+      double* out = c->d_stage + (size_t)(s - s0) * n;
+      if (c->is_double)
+        k_fetch_field<double><<<grid, B, 0, c->stream>>>(c->md_d[mesh].U, what * 6, c->md_d[mesh].ES, c->md_d[mesh].PS,
+                                                         s, h.d_new_of_old, (int)h.K, out);
+      else
+        k_fetch_field<float><<<grid, B, 0, c->stream>>>(c->md_f[mesh].U, what * 6, c->md_f[mesh].ES, c->md_f[mesh].PS,
+                                                        s, h.d_new_of_old, (int)h.K, out);
+    }
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(dst, c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(dst, c->d_stage, (size_t)n * (s1 - s0) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   } else if (what == DG_TRACE_X || what == DG_TRACE_Z) {
     const long long steps = std::min(c->t, h.steps);
     const long long n = steps * h.n_rec;

@@ -22,7 +22,6 @@ ERRORS = {0: "DG_OK", -1: "DG_ERR_ARG", -2: "DG_ERR_CUDA", -3: "DG_ERR_NOMEM", -
           -5: "DG_ERR_NONFINITE", -6: "DG_ERR_STATE", -7: "DG_ERR_UNSUPPORTED", -8: "DG_ERR_NODEVICE",
           -9: "DG_ERR_ORIENTATION", -10: "DG_ERR_TIMEOUT"}
 
-# exported symbols of include/dg_gpu.h (checked by the CPU tests)
 def _ptr(a):
     """Address of a host buffer: a numpy array or anything with data_ptr() (e.g. pinned memory)."""
     if hasattr(a, "data_ptr"):
@@ -32,6 +31,7 @@ def _ptr(a):
     return a.ctypes.data
 
 
+# exported symbols of include/dg_gpu.h (checked by the CPU tests)
 EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_async", "dg_gpu_synchronize", "dg_gpu_step_timed", "dg_gpu_step_profiled",
            "dg_gpu_fetch_traces", "dg_gpu_fetch", "dg_gpu_load",
            "dg_gpu_reset", "dg_gpu_set_wavelet", "dg_gpu_flush_l2", "dg_gpu_stats_get", "dg_gpu_steps_done",
@@ -41,8 +41,10 @@ EXPORTS = ["dg_gpu_default_opts", "dg_gpu_init", "dg_gpu_step", "dg_gpu_step_asy
            "dg_gpu_context_stream"]
 # parts of a half step (dg_gpu_half_step_part)
 PART_ALL, PART_BOUNDARY, PART_INTERIOR = 0, 1, 2
-# every mesh of the context at once (dg_gpu_fetch_traces, dg_gpu_set_wavelet)
+# every mesh of the context at once (dg_gpu_fetch_traces, dg_gpu_set_wavelet), every shot of a
+# mesh at once (dg_gpu_fetch of a field)
 ALL_MESHES = -1
+ALL_SHOTS = -1
 
 
 def energy_noalloc(device: int, K: int, fields, jacobi, A, inverV: np.ndarray, out, stream=None) -> None:
@@ -328,7 +330,9 @@ class Engine:
         if isinstance(what, str):
             what = FIELDS.get(what, {"trace_x": TRACE_X, "trace_z": TRACE_Z, "energy": ENERGY}.get(what, -99))
         inf = self.info[mesh]
-        if what in (VX, VZ, TXX, TZZ, TXZ):
+        if what in (VX, VZ, TXX, TZZ, TXZ) and shot == ALL_SHOTS:
+            out = np.empty((inf["S"], inf["K"] * 6))
+        elif what in (VX, VZ, TXX, TZZ, TXZ):
             out = np.empty(inf["K"] * 6)
         elif what in (TRACE_X, TRACE_Z):
             out = np.empty((min(self.steps_done, inf["T"]), inf["R"]))

@@ -163,7 +163,9 @@ int dg_gpu_fetch_traces(dg_gpu_ctx *ctx, int mesh, long t0, long n, double *dst_
 
 /* Copy one item of one mesh/shot to host memory `dst`, in the reference's layout:
  * fields as double[K][Np] in the caller's element numbering, traces as double[steps][n_rec],
- * energy as one double. */
+ * energy as one double.  For a field, shot = DG_ALL_SHOTS copies every shot of the mesh,
+ * double[n_shots][K][Np], with one synchronisation. */
+#define DG_ALL_SHOTS (-1)
 int dg_gpu_fetch(dg_gpu_ctx *ctx, int what, int mesh, int shot, double *dst);
 
 /* Overwrite one field of one mesh/shot from host memory (checkpoint restore); layout as fetch. */

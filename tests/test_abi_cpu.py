@@ -36,3 +36,19 @@ def test_error_strings_without_device():
     lib = pkg.engine.lib()
     for code in (0, -1, -2, -3, -4, -5, -6, -7, -8, -9):
         assert lib.dg_gpu_strerror(code)
+
+
+def test_binding_constants_equal_header():
+    """Every #define of dg_gpu.h the Python binding restates has the header's value."""
+    with open(os.path.join(ROOT, "include", "dg_gpu.h")) as f:
+        defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"^#define (DG_\w+) \(?(-?\d+)L?\)?", f.read(), re.M)}
+    e = pkg.engine
+    same = {"DG_FP64_REF": e.FP64_REF, "DG_FP64": e.FP64, "DG_FP32": e.FP32, "DG_FP32_KAHAN": e.FP32_KAHAN,
+            "DG_VX": e.VX, "DG_VZ": e.VZ, "DG_TXX": e.TXX, "DG_TZZ": e.TZZ, "DG_TXZ": e.TXZ,
+            "DG_TRACE_X": e.TRACE_X, "DG_TRACE_Z": e.TRACE_Z, "DG_ENERGY": e.ENERGY,
+            "DG_ALL_MESHES": e.ALL_MESHES, "DG_ALL_SHOTS": e.ALL_SHOTS, "DG_PART_ALL": e.PART_ALL,
+            "DG_PART_BOUNDARY": e.PART_BOUNDARY, "DG_PART_INTERIOR": e.PART_INTERIOR}
+    for name, value in same.items():
+        assert defs[name] == value, name
+    for code, name in e.ERRORS.items():
+        assert defs[name] == code, name

@@ -137,3 +137,16 @@ def test_async_steps_equal_synchronous_steps(meshes, precision, wave):
             assert e.steps_done == 150
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_fetch_every_shot_at_once(meshes, precision):
+    """DG_ALL_SHOTS: one call returns a field of every shot of a mesh, equal to the per-shot calls."""
+    with eng.Engine(meshes[3], precision) as e:     # 16 shots
+        e.step(60)
+        for f in ("Vx", "Txz"):
+            every = e.fetch(f, 0, eng.ALL_SHOTS)
+            assert every.shape == (16, e.info[0]["K"] * 6)
+            for s in range(16):
+                assert np.array_equal(every[s], e.fetch(f, 0, s))
+        assert np.abs(every).max() > 0

@@ -3,10 +3,13 @@
 // dg_gpu_energy_noalloc computes the same FP64 energy as dg_gpu_fetch(DG_ENERGY) from fields the
 // caller already holds in device memory, and keeps its partial sums in a file-scope static
 // device array instead of a cudaMalloc'd buffer.  Host code must not use g_partials' name as a
-// device address: it is a host-side stand-in.  The device address is looked up once per device
-// with cudaGetSymbolAddress and handed to the kernels.
+// device address: it is a host-side stand-in.  The device address is looked up with
+// cudaGetSymbolAddress, with the device current, on the first call on each device and again
+// whenever that device's current context is no longer the one the address was taken in (after
+// a cudaDeviceReset by the host program), and handed to the kernels.
 #include "dg_gpu.h"
 
+#include <cuda.h>  // CUcontext and CUresult only: the driver call is found at run time
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -25,7 +28,11 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_partials[kMaxPartials];
 
 std::mutex g_mu;
-double* g_addr[kMaxDevices] = {};
+struct Slot {
+  void* ctx = nullptr;     // the context the address was taken in
+  double* addr = nullptr;  // g_partials' device address there
+};
+Slot g_slot[kMaxDevices];
 
 struct Mass {
   double M[36];  // reference mass matrix inv(V V^T) = inverV^T inverV
@@ -95,20 +102,85 @@ int fail(int code, const char* msg) {
   return code;
 }
 
-// Device address of g_partials on `device` (made current); looked up on the first call only.
+int cuda_fail(const char* what, cudaError_t e) {
+  dg::set_last_error((std::string(what) + ": " + cudaGetErrorString(e)).c_str());
+  return DG_ERR_CUDA;
+}
+
+// The current driver context as an opaque key, or null where the driver entry point is not
+// available (then the address is taken once per device and kept).
+void* current_context() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  static GetCurrent fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (GetCurrent) nullptr;
+    return reinterpret_cast<GetCurrent>(p);
+  }();
+  CUcontext ctx = nullptr;
+  if (!fn || fn(&ctx) != CUDA_SUCCESS) return nullptr;
+  return ctx;
+}
+
+// Device address of g_partials on `device`, which the caller has made current.  Taken on the
+// first call on the device and again when the device's context has changed since.
 int scratch_on(int device, double** addr) {
+  void* ctx = current_context();
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[device]) {
-    if (cudaSetDevice(device) != cudaSuccess) return fail(DG_ERR_NODEVICE, "cannot make the device current");
+  Slot& sl = g_slot[device];
+  if (!sl.addr || sl.ctx != ctx) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_partials);
-    if (e != cudaSuccess || !p) {
-      dg::set_last_error((std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)).c_str());
-      return DG_ERR_CUDA;
-    }
-    g_addr[device] = static_cast<double*>(p);
+    if (e != cudaSuccess) return cuda_fail("cudaGetSymbolAddress", e);
+    if (!p) return fail(DG_ERR_CUDA, "cudaGetSymbolAddress gave no address");
+    sl.addr = static_cast<double*>(p);
+    sl.ctx = ctx;
   }
-  *addr = g_addr[device];
+  *addr = sl.addr;
+  return DG_OK;
+}
+
+// Makes `device` current for the life of the object and puts the caller's device back after.
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DeviceScope(int device) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != device) err = cudaSetDevice(device);
+  }
+  ~DeviceScope() {
+    int now = -1;
+    if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+  }
+};
+
+int energy_on_device(int device, long K, const double* Vx, const double* Vz, const double* Txx,
+                     const double* Tzz, const double* Txz, const double* Jacobi, const double* A,
+                     const double* inverV, double* out, void* stream) {
+  double* partials = nullptr;
+  int rc = scratch_on(device, &partials);
+  if (rc) return rc;
+  Mass mass;
+  for (int i = 0; i < 6; i++)
+    for (int k = 0; k < 6; k++) {
+      double a = 0;
+      for (int q = 0; q < 6; q++) a += inverV[q * 6 + i] * inverV[q * 6 + k];
+      mass.M[i * 6 + k] = a;
+    }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int blocks = (int)((K + kBlock - 1) / kBlock);
+  // launched through cudaLaunchKernel so each launch's own status is checked and an error the
+  // host program left pending in the runtime is neither returned nor cleared here
+  void* a1[] = {&mass, &K, &Vx, &Vz, &Txx, &Tzz, &Txz, &Jacobi, &A, &partials};
+  cudaError_t e = cudaLaunchKernel((const void*)k_energy_partials, dim3(blocks), dim3(kBlock), a1, 0, st);
+  if (e != cudaSuccess) return cuda_fail("dg_gpu_energy_noalloc: partial sums", e);
+  void* a2[] = {&partials, &blocks, &out};
+  e = cudaLaunchKernel((const void*)k_energy_finish, dim3(1), dim3(1024), a2, 0, st);
+  if (e != cudaSuccess) return cuda_fail("dg_gpu_energy_noalloc: final sum", e);
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail("dg_gpu_energy_noalloc", e);
   return DG_OK;
 }
 
@@ -123,26 +195,7 @@ extern "C" int dg_gpu_energy_noalloc(int device, long K, const double* Vx, const
     return fail(DG_ERR_ARG, "K exceeds DG_NOALLOC_MAX_ELEMENTS (4,194,304): the static scratch is too small");
   if (!Vx || !Vz || !Txx || !Tzz || !Txz || !Jacobi || !A || !inverV || !out)
     return fail(DG_ERR_ARG, "null pointer");
-  double* partials = nullptr;
-  int rc = scratch_on(device, &partials);
-  if (rc) return rc;
-  if (cudaSetDevice(device) != cudaSuccess) return fail(DG_ERR_NODEVICE, "cannot make the device current");
-  Mass mass;
-  for (int i = 0; i < 6; i++)
-    for (int k = 0; k < 6; k++) {
-      double a = 0;
-      for (int q = 0; q < 6; q++) a += inverV[q * 6 + i] * inverV[q * 6 + k];
-      mass.M[i * 6 + k] = a;
-    }
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int blocks = (int)((K + kBlock - 1) / kBlock);
-  k_energy_partials<<<blocks, kBlock, 0, st>>>(mass, K, Vx, Vz, Txx, Tzz, Txz, Jacobi, A, partials);
-  k_energy_finish<<<1, 1024, 0, st>>>(partials, blocks, out);
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) {
-    dg::set_last_error((std::string("dg_gpu_energy_noalloc: ") + cudaGetErrorString(e)).c_str());
-    return DG_ERR_CUDA;
-  }
-  return DG_OK;
+  DeviceScope scope(device);
+  if (scope.err != cudaSuccess) return fail(DG_ERR_NODEVICE, "cannot make the device current");
+  return energy_on_device(device, K, Vx, Vz, Txx, Tzz, Txz, Jacobi, A, inverV, out, stream);
 }

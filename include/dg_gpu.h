@@ -283,12 +283,16 @@ int dg_gpu_debug_stall_wave(dg_gpu_ctx *ctx, int unit);
  * Scratch: a file-scope static device array of DG_NOALLOC_MAX_ELEMENTS/256 doubles (128 KiB),
  * which every GPU that loads this library holds until the process exits.  K beyond
  * DG_NOALLOC_MAX_ELEMENTS is rejected with DG_ERR_ARG before anything runs.  The first call on a
- * device makes that device current and looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share
- * the array: calls that overlap on the GPU (other streams, other host threads) race and give
- * wrong results.  Each call overwrites every partial it reads, so nothing has to start at zero.
- * `stream` is a cudaStream_t (NULL: the default stream); the call returns after the result is
- * in `out`. */
+ * device looks up the array's device address there (cudaGetSymbolAddress), with that device
+ * current; a later call looks it up again only if the device's context has changed since (a
+ * cudaDeviceReset by the host program).  Make the first call on each device, and the first one
+ * after such a reset, before any stream capture.  Each call works on `device` and gives the
+ * calling thread its previous current device back before it returns, on every path.  Launch
+ * errors are read from the launches themselves: an error the host program left pending in the
+ * CUDA runtime is neither returned nor cleared.  All calls share the array: calls that overlap
+ * on the GPU (other streams, other host threads) race and give wrong results.  Each call
+ * overwrites every partial it reads, so nothing has to start at zero.  `stream` is a
+ * cudaStream_t (NULL: the default stream); the call returns after the result is in `out`. */
 int dg_gpu_energy_noalloc(int device, long K, const double *Vx, const double *Vz, const double *Txx,
                           const double *Tzz, const double *Txz, const double *Jacobi, const double *A,
                           const double *inverV, double *out, void *stream);

@@ -12,11 +12,7 @@
 #include "dg_gpu.h"
 #include "dg_aux.cuh"
 #include "dg_common.cuh"
-#include "dg_step_generic.cuh"
-#include "dg_step_multi.cuh"
-#include "dg_step_ref.cuh"
-#include "dg_step_wave.cuh"
-#include "dg_step_x2.cuh"
+#include "dg_kernels.cuh"
 
 #include <omp.h>
 #include <parallel/algorithm>
@@ -705,13 +701,18 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
   return DG_OK;
 }
 
+int wave_resident(dg_gpu_ctx* c, int& per_sm);
+
+// Sets the ticket counter to the step the counters hold, for a launch grid of G blocks.
+__global__ void k_wave_sync(const Counters* __restrict__ ctr, unsigned long long* tickets, unsigned G) {
+  *tickets = (unsigned long long)ctr->v * G;
+}
+
 // Schedule of the wavefront step for the current block size.  A unit is one warp's 32 threads of
 // the element range (thread g works on element g / H, H = shots / 2); the wait list holds, per unit, the
 // distinct units covering one of its elements or a neighbour of one; the lag L (in blocks) covers
 // the unit bandwidth plus a margin of about 60 % of the resident warps, so a stress update
 // seldom waits.  Receivers are listed under every unit that covers their element.
-template <bool KAHAN> int wave_resident(dg_gpu_ctx* c, int& per_sm);
-
 int build_wave(dg_gpu_ctx* c) {
   const MeshHostInfo& h = c->mi[0];
   // two-shot layout: H = S/2 threads per element; one-shot layout: thread p owns elements 2p and
@@ -816,7 +817,7 @@ int build_wave(dg_gpu_ctx* c) {
   w.inv_G = ~0ULL / (unsigned long long)c->blocks_v;
   if (c->wave_persistent) {
     int per_sm = 0;
-    if ((rc = c->kahan ? wave_resident<true>(c, per_sm) : wave_resident<false>(c, per_sm))) return rc;
+    if ((rc = wave_resident(c, per_sm))) return rc;
     if (per_sm < 1) return fail(DG_ERR_UNSUPPORTED, "the persistent wavefront kernel does not fit an SM");
     c->blocks_p = std::min(c->blocks_v, per_sm * c->num_sms);
   }
@@ -879,52 +880,22 @@ int launch_k(dg_gpu_ctx* c, void (*kernel)(K...), dim3 grid, dim3 block, A&&... 
     if (rc_) return rc_;                                      \
   } while (0)
 
-template <bool KAHAN>
 int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid, bool hv = true, bool ht = true) {
   const dim3 bl(c->block), gv(c->blocks_v), gt(c->blocks_t);
-  cudaStream_t st = c->stream;
-  switch (c->x2 + (c->x2pm ? 1000 : 0)) {
-    case 1:  // one shot: two elements per thread
-      if (hv) DG_LAUNCH(k_velocity_x2e<KAHAN>, gv, c->ops2, c->md_f[0], c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH(k_stress_x2e<KAHAN>, gt, c->ops2, c->md_f[0], c->d_ctr);
-      break;
-#define DG_X2(SS)                                                                      \
-  case SS:                                                                             \
-    if (hv) DG_LAUNCH((k_velocity_x2<SS, KAHAN>), gv, c->ops2, c->md_f[0], c->d_ctr);   \
-    if (mid) CK(cudaEventRecord(mid, st));                                             \
-    if (ht) DG_LAUNCH((k_stress_x2<SS, KAHAN>), gt, c->ops2, c->md_f[0], c->d_ctr);     \
-    break;
-#define DG_X2PM(SS)                                                                          \
-  case 1000 + SS:                                                                            \
-    if (hv) DG_LAUNCH((k_velocity_x2<SS, KAHAN, true>), gv, c->ops2, c->md_f[0], c->d_ctr);   \
-    if (mid) CK(cudaEventRecord(mid, st));                                                   \
-    if (ht) DG_LAUNCH((k_stress_x2<SS, KAHAN, true>), gt, c->ops2, c->md_f[0], c->d_ctr);     \
-    break;
-    DG_X2(2) DG_X2(4) DG_X2(6) DG_X2(8) DG_X2(10) DG_X2(12) DG_X2(14) DG_X2(16) DG_X2(32) DG_X2(64) DG_X2(128)
-    DG_X2PM(2) DG_X2PM(4) DG_X2PM(6) DG_X2PM(8) DG_X2PM(10) DG_X2PM(12) DG_X2PM(14) DG_X2PM(16)
-#undef DG_X2PM
-#undef DG_X2
-    default:
-      return fail(DG_ERR_UNSUPPORTED, "no two-shot kernel for this shot count");
-  }
+  const HalfPair<X2Fn> k = kernels_packed(c->x2, c->kahan, c->x2pm);
+  if (!k.v) return fail(DG_ERR_UNSUPPORTED, "no two-shot kernel for this shot count");
+  if (hv) DG_LAUNCH(k.v, gv, c->ops2, c->md_f[0], c->d_ctr);
+  if (mid) CK(cudaEventRecord(mid, c->stream));
+  if (ht) DG_LAUNCH(k.s, gt, c->ops2, c->md_f[0], c->d_ctr);
   return DG_OK;
 }
 
 // resident blocks of the persistent wavefront kernel for the current block size
-template <bool KAHAN>
 int wave_resident(dg_gpu_ctx* c, int& per_sm) {
-  cudaError_t e = cudaErrorInvalidValue;
   per_sm = 0;
-  switch (c->x2) {
-#define DG_WO(SS, LAYOUT) \
-  case SS: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_wave_p<LAYOUT, KAHAN>, c->block, 0); break;
-    DG_WO(1, WaveOneShot)
-    DG_WO(2, WaveTwoShots<2>) DG_WO(4, WaveTwoShots<4>) DG_WO(8, WaveTwoShots<8>) DG_WO(16, WaveTwoShots<16>)
-    DG_WO(32, WaveTwoShots<32>) DG_WO(64, WaveTwoShots<64>) DG_WO(128, WaveTwoShots<128>)
-#undef DG_WO
-    default: break;
-  }
+  const WaveFn k = kernel_wave(c->x2, c->kahan, true);
+  if (!k) return fail(DG_ERR_UNSUPPORTED, "no wavefront step for this shot count");
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, c->block, 0);
   if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __LINE__);
   return DG_OK;
 }
@@ -932,34 +903,18 @@ int wave_resident(dg_gpu_ctx* c, int& per_sm) {
 // shot counts with a wavefront step instance
 bool wave_supported(int S) { return S == 2 || S == 4 || S == 8 || S == 16 || S == 32 || S == 64 || S == 128; }
 
-template <bool KAHAN>
 int launch_wave(dg_gpu_ctx* c) {
-  const dim3 bl(c->block), g(c->blocks_v), gp(c->blocks_p);
-  switch (c->x2) {
-#define DG_WV(SS, LAYOUT)                                                                          \
-  case SS:                                                                                        \
-    if (c->wave_persistent)                                                                       \
-      k_step_wave_p<LAYOUT, KAHAN><<<gp, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr); \
-    else                                                                                          \
-      k_step_wave<LAYOUT, KAHAN><<<g, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr);  \
-    break;
-    DG_WV(1, WaveOneShot)
-#define DG_WV2(SS) DG_WV(SS, WaveTwoShots<SS>)
-    DG_WV2(2) DG_WV2(4) DG_WV2(8) DG_WV2(16) DG_WV2(32) DG_WV2(64) DG_WV2(128)
-#undef DG_WV2
-#undef DG_WV
-    default:
-      return fail(DG_ERR_UNSUPPORTED, "no wavefront step for this shot count");
-  }
+  const WaveFn k = kernel_wave(c->x2, c->kahan, c->wave_persistent);
+  if (!k) return fail(DG_ERR_UNSUPPORTED, "no wavefront step for this shot count");
+  const dim3 bl(c->block), g(c->wave_persistent ? c->blocks_p : c->blocks_v);
+  k<<<g, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr);
   return DG_OK;
 }
 
 // resident blocks of the persistent batch kernel for the current block size
 int mx_resident(dg_gpu_ctx* c) {
   int per_sm = 0;
-  cudaError_t e = c->kahan
-      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_mx_p<true>, c->block, 0)
-      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_mx_p<false>, c->block, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_batch_persistent(c->kahan), c->block, 0);
   if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __LINE__);
   if (per_sm < 1) return fail(DG_ERR_UNSUPPORTED, "the persistent batch kernel does not fit on an SM");
   c->blocks_mxp = per_sm * c->num_sms;
@@ -973,7 +928,7 @@ int launch_mx_p(dg_gpu_ctx* c, int nsteps) {
   CK(cudaMemsetAsync(c->d_mxbar, 0, sizeof(unsigned), c->stream));
   const MeshDev<float>* tab = c->d_tab_f;
   void* args[] = {&c->ops_f, &c->ops2, &tab, &L, &c->d_ctr, &nsteps};
-  const void* fn = c->kahan ? (const void*)k_step_mx_p<true> : (const void*)k_step_mx_p<false>;
+  const void* fn = (const void*)kernel_batch_persistent(c->kahan);
   CK(cudaLaunchCooperativeKernel(fn, dim3(c->blocks_mxp), dim3(c->block), args, 0, c->stream));
   return DG_OK;
 }
@@ -986,36 +941,23 @@ int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid =
   const dim3 gv(c->blocks_v), gt(c->blocks_t);
   cudaStream_t st = c->stream;
   if (before_t) CK(cudaEventRecord(before_t, st));
+  // the two launches of a step of family F (mesh table and block table for a batch)
+#define DG_TWO(F, OPS, MESH, TAB, BTV, BTT)                                  \
+  do {                                                                       \
+    if (hv) DG_LAUNCH(F.v, gv, OPS, MESH, TAB, BTV, c->d_ctr);               \
+    if (mid) CK(cudaEventRecord(mid, st));                                   \
+    if (ht) DG_LAUNCH(F.s, gt, OPS, MESH, TAB, BTT, c->d_ctr);               \
+  } while (0)
   if (c->precision == DG_FP64_REF) {
-    if (c->multi) {
-      if (hv) DG_LAUNCH((k_velocity_ref<true, false>), gv, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress_ref<true, false>), gt, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
-    } else {
-      const MeshDev<double>* no_tab = nullptr;
-      const int2* no_btab = nullptr;
-      if (c->ref_otf) {
-        if (hv) DG_LAUNCH((k_velocity_ref<false, true>), gv, c->ops_d, c->md_d[0], no_tab, no_btab, c->d_ctr);
-        if (mid) CK(cudaEventRecord(mid, st));
-        if (ht) DG_LAUNCH((k_stress_ref<false, true>), gt, c->ops_d, c->md_d[0], no_tab, no_btab, c->d_ctr);
-      } else {
-        if (hv) DG_LAUNCH((k_velocity_ref<false, false>), gv, c->ops_d, c->md_d[0], no_tab, no_btab, c->d_ctr);
-        if (mid) CK(cudaEventRecord(mid, st));
-        if (ht) DG_LAUNCH((k_stress_ref<false, false>), gt, c->ops_d, c->md_d[0], no_tab, no_btab, c->d_ctr);
-      }
-    }
+    const HalfPair<GenFn<double>> k = kernels_reference(c->multi, c->ref_otf);
+    if (c->multi) DG_TWO(k, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_btab_t);
+    else DG_TWO(k, c->ops_d, c->md_d[0], (const MeshDev<double>*)nullptr, (const int2*)nullptr, (const int2*)nullptr);
   } else if (c->is_double) {
-    if (c->multi) {
-      if (hv) DG_LAUNCH((k_velocity<double, false, true>), gv, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress<double, false, true>), gt, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_t, c->d_ctr);
-    } else {
-      if (hv) DG_LAUNCH((k_velocity<double, false, false>), gv, c->ops_d, c->md_d[0], (const MeshDev<double>*)nullptr, (const int2*)nullptr, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress<double, false, false>), gt, c->ops_d, c->md_d[0], (const MeshDev<double>*)nullptr, (const int2*)nullptr, c->d_ctr);
-    }
+    const HalfPair<GenFn<double>> k = kernels_fp64(c->multi);
+    if (c->multi) DG_TWO(k, c->ops_d, c->md_d[0], c->d_tab_d, c->d_btab_v, c->d_btab_t);
+    else DG_TWO(k, c->ops_d, c->md_d[0], (const MeshDev<double>*)nullptr, (const int2*)nullptr, (const int2*)nullptr);
   } else if (c->wave) {  // the whole step in one launch: it is timed as the "velocity" interval
-    int rc = c->kahan ? launch_wave<true>(c) : launch_wave<false>(c);
+    int rc = launch_wave(c);
     if (rc) return rc;
     if (mid) CK(cudaEventRecord(mid, st));
   } else if (c->mx && c->mx_persistent) {  // the whole step in one launch, timed as the "velocity" interval
@@ -1023,39 +965,19 @@ int launch_step(dg_gpu_ctx* c, cudaEvent_t before_t = nullptr, cudaEvent_t mid =
     if (rc) return rc;
     if (mid) CK(cudaEventRecord(mid, st));
   } else if (c->mx) {
-    if (c->kahan) {
-      if (hv) DG_LAUNCH((k_velocity_mx<true>), gv, c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress_mx<true>), gt, c->ops_f, c->ops2, c->d_tab_f, c->d_btab_t, c->d_ctr);
-    } else {
-      if (hv) DG_LAUNCH((k_velocity_mx<false>), gv, c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress_mx<false>), gt, c->ops_f, c->ops2, c->d_tab_f, c->d_btab_t, c->d_ctr);
-    }
+    const HalfPair<MxFn> k = kernels_batch(c->kahan);
+    if (hv) DG_LAUNCH(k.v, gv, c->ops_f, c->ops2, c->d_tab_f, c->d_btab_v, c->d_ctr);
+    if (mid) CK(cudaEventRecord(mid, st));
+    if (ht) DG_LAUNCH(k.s, gt, c->ops_f, c->ops2, c->d_tab_f, c->d_btab_t, c->d_ctr);
   } else if (c->x2) {
-    int rc = c->kahan ? launch_x2<true>(c, mid, hv, ht) : launch_x2<false>(c, mid, hv, ht);
+    int rc = launch_x2(c, mid, hv, ht);
     if (rc) return rc;
-  } else if (c->kahan) {
-    if (c->multi) {
-      if (hv) DG_LAUNCH((k_velocity<float, true, true>), gv, c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress<float, true, true>), gt, c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_t, c->d_ctr);
-    } else {
-      if (hv) DG_LAUNCH((k_velocity<float, true, false>), gv, c->ops_f, c->md_f[0], (const MeshDev<float>*)nullptr, (const int2*)nullptr, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress<float, true, false>), gt, c->ops_f, c->md_f[0], (const MeshDev<float>*)nullptr, (const int2*)nullptr, c->d_ctr);
-    }
   } else {
-    if (c->multi) {
-      if (hv) DG_LAUNCH((k_velocity<float, false, true>), gv, c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress<float, false, true>), gt, c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_t, c->d_ctr);
-    } else {
-      if (hv) DG_LAUNCH((k_velocity<float, false, false>), gv, c->ops_f, c->md_f[0], (const MeshDev<float>*)nullptr, (const int2*)nullptr, c->d_ctr);
-      if (mid) CK(cudaEventRecord(mid, st));
-      if (ht) DG_LAUNCH((k_stress<float, false, false>), gt, c->ops_f, c->md_f[0], (const MeshDev<float>*)nullptr, (const int2*)nullptr, c->d_ctr);
-    }
+    const HalfPair<GenFn<float>> k = kernels_fp32(c->kahan, c->multi);
+    if (c->multi) DG_TWO(k, c->ops_f, c->md_f[0], c->d_tab_f, c->d_btab_v, c->d_btab_t);
+    else DG_TWO(k, c->ops_f, c->md_f[0], (const MeshDev<float>*)nullptr, (const int2*)nullptr, (const int2*)nullptr);
   }
+#undef DG_TWO
   CK(cudaGetLastError());
   if (after) CK(cudaEventRecord(after, st));
   return DG_OK;
@@ -1525,16 +1447,16 @@ static int ensure_flush(dg_gpu_ctx* c) {
   return DG_OK;
 }
 
+// The staging buffer of at least `elems` doubles.  A larger one is allocated before the smaller
+// one is released, so a failed allocation leaves the old buffer in place and the call fails.
 static int ensure_stage(dg_gpu_ctx* c, size_t elems) {
-  if (elems <= c->stage_elems) return DG_OK;
-  c->release(c->d_stage);  // the smaller one (after the stream has finished with it)
-  c->d_stage = nullptr;
-  c->stage_elems = 0;
+  if (c->d_stage && elems <= c->stage_elems) return DG_OK;
   double* p = nullptr;
-  int rc = c->alloc(&p, elems);
+  int rc = c->alloc(&p, std::max(elems, c->stage_elems));
   if (rc) return rc;
+  c->release(c->d_stage);  // the smaller one (after the stream has finished with it)
   c->d_stage = p;
-  c->stage_elems = elems;
+  c->stage_elems = std::max(elems, c->stage_elems);
   return DG_OK;
 }
 
@@ -1721,6 +1643,8 @@ int dg_gpu_fetch(dg_gpu_ctx* c, int what, int mesh, int shot, double* dst) {
     const long long steps = std::min(c->t, h.steps);
     const long long n = steps * h.n_rec;
     if (n > 0) {
+      int rc = ensure_stage(c, (size_t)n);
+      if (rc) return rc;
       const int grid = (int)((n + B - 1) / B);
       const int comp = what - DG_TRACE_X;
       if (c->is_double)
@@ -1753,6 +1677,8 @@ int dg_gpu_load(dg_gpu_ctx* c, int what, int mesh, int shot, const double* src) 
   if (what < DG_VX || what > DG_TXZ) return fail(DG_ERR_STATE, "only fields can be loaded");
   CK(cudaSetDevice(c->device));
   const long long n = h.K * 6;
+  int rc = ensure_stage(c, (size_t)n);
+  if (rc) return rc;
   CK(cudaMemcpyAsync(c->d_stage, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   const int B = 256, grid = (int)((n + B - 1) / B);
   if (c->is_double)

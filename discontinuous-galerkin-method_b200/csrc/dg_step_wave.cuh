@@ -143,11 +143,6 @@ __device__ __forceinline__ void wait_units(const Wave& w, int k, unsigned id) {
   __syncwarp();
 }
 
-// Sets the ticket counter to the step the counters hold, for a launch grid of G blocks.
-__global__ void k_wave_sync(const Counters* __restrict__ ctr, unsigned long long* tickets, unsigned G) {
-  *tickets = (unsigned long long)ctr->v * G;
-}
-
 // The work of ticket tau in step t: the velocity half of the units of block tau and the stress
 // half of the units of block tau - L (each warp one unit of each).
 template <class Layout, bool KAHAN>

@@ -1,6 +1,6 @@
 """Generate the golden fixtures from the reference's own C code.
 
-Run in a container that has the reference tree (default /root/reference) and the compiled
+Run in a container that has the reference tree (default $DG_REFERENCE_ROOT, else /root/reference) and the compiled
 harness (``make -C oracle ref``)::
 
     python tests/golden/make_golden.py [--ref /root/reference]
@@ -78,7 +78,7 @@ def make(name, w, ref_root):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("DG_REFERENCE_ROOT", "/root/reference"))
     args = ap.parse_args()
     for name, fn in CASES.items():
         w = fn(pkg.workloads)

@@ -4,10 +4,10 @@
 One bench step = one time step of the whole workload: sponge, source, velocity half-step,
 stress half-step and receiver record for every element, shot and mesh.  The default workload is
 the multi-shot batch: a layered elastic mesh of 200,000 triangles advanced for 64 shots at once
-in FP32 (shots innermost).  Beside it the line reports the plain FP64 path (one shot, L2 flushed
-between steps), the FP32-vs-FP64 trace error, the roofline of the dominant kernel, an end-to-end
-figure through the public API with host buffers, and the reference's own CPU code timed on this
-host.
+in FP32 (shots innermost).  Beside it the line reports the plain FP64 path on one shot of the same
+mesh (timed exactly as the batch, and again with L2 flushed before every step), the FP32-vs-FP64
+trace error, the roofline of the dominant kernel, an end-to-end figure through the public API
+with host buffers, and the reference's own CPU code timed on this host.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
                     [--precision fp32|fp32_kahan|fp64]
@@ -61,6 +61,9 @@ WORKLOADS = {
     # name: (constructor(steps, rank) -> Workload or list of Workloads, description)
     "multishot": (lambda steps, rank: pkg().workloads.layered_multishot(steps=steps, shot_phase=(rank % 16) / 16.0),
                   "multi-shot layered elastic batch: 200,000 triangles x 64 shots"),
+    # one shot of that mesh: the plain FP64 path's workload, for profiling it on its own
+    "layered1": (lambda steps, rank: one_shot(pkg().workloads.layered_multishot(steps=steps)),
+                 "layered elastic mesh of the multi-shot batch, 200,000 triangles, 1 shot"),
     "slope": (lambda steps, rank: pkg().workloads.coupled_slope(steps=steps),
               "coupled acoustic-elastic slope: ~400,000 triangles, 1 shot"),
     "random": (lambda steps, rank: pkg().workloads.random_medium(steps=steps),
@@ -343,19 +346,25 @@ def run_ours(args):
     total_ms = ev0.elapsed_time(ev1)
     launches = e.stats()["launches"]
     value, t_max = weak_scaling_value(dof_step, K_steps, total_ms, world, dist, device)
-    # then K more steps with events around every launch: the per-kernel times of the roofline
-    mv, ms, _ = e.step_profiled(K_steps)
-
-    t_vel, t_str = float(np.mean(mv)), float(np.mean(ms))
     names = eng.KERNEL_NAMES[st["kernel_family"]]
-    if names[1] is None:  # the whole step in one launch (timed as the first interval)
-        dom = (names[0], bytes_step, t_vel)
-        kernels = {names[0]: {"ms": t_vel, "GBs": bytes_step / (t_vel * 1e-3) / 1e9}}
+    if names[1] is None:
+        # the whole step in one launch (or the whole run in one persistent launch): the kernel's
+        # time per step is the timed region's, on the stream it runs on
+        t_one = total_ms / K_steps
+        dom = (names[0], bytes_step, t_one)
+        kernels = {names[0]: {"ms": t_one, "GBs": bytes_step / (t_one * 1e-3) / 1e9}}
+        time_source = ("the timed region: CUDA events on the context's stream around the %d-step call, "
+                       "%d launches of %s" % (K_steps, launches, names[0]))
     else:
+        # two launches a step: K more steps with events around every launch give each kernel's time
+        mv, ms, _ = e.step_profiled(K_steps)
+        t_vel, t_str = float(np.mean(mv)), float(np.mean(ms))
         b_vel, b_str = kernel_bytes(ws, args.precision)
         dom = (names[1], b_str, t_str) if t_str >= t_vel else (names[0], b_vel, t_vel)
         kernels = {names[0]: {"ms": t_vel, "GBs": b_vel / (t_vel * 1e-3) / 1e9},
                    names[1]: {"ms": t_str, "GBs": b_str / (t_str * 1e-3) / 1e9}}
+        time_source = ("a separate run of %d steps after the timed region, CUDA events around every launch"
+                       % K_steps)
     achieved = dom[1] / (dom[2] * 1e-3) / 1e9
     traffic = read_traffic(args.workload, dom[0])
     S_tot = sum(x.shots for x in ws)
@@ -452,13 +461,27 @@ def run_ours(args):
                                 "field value); the long-run accuracy of this workload is checked in "
                                 "tests/test_gpu_fullsize.py" % acc_steps}
 
-    # ---- plain FP64 path on the first mesh: one shot, L2 flushed before every step ----------
+    # ---- plain FP64 path on the first mesh, one shot, timed two ways ------------------------
+    # (1) exactly as `value`: one dg_gpu_step(K) call (CUDA graphs), events on the context's stream
+    #     around it, no flush (a one-shot FP64 state of this mesh may sit in L2 between steps);
+    # (2) events around every launch with a 256 MB write before every step, so each step starts
+    #     from a cold L2 (the state streams from HBM, as it does for the batch, whose 1.5 GB
+    #     cannot stay in L2)
     s1 = P.host.build_setup(one_shot(ws[0]), full=False, n_steps=table)
     with eng.Engine(eng.mesh_from_setup(s1, with_ref_ops=False), "fp64", device=device) as e1:
         e1.step(W_steps)
-        _, _, tot1 = e1.step_profiled(K_steps, flush_l2=True)
         st1 = e1.stats()
+        s64 = e1.stream()
+        torch.cuda.synchronize(device)
+        ev0.record(s64)
+        e1.step(K_steps)
+        ev1.record(s64)
+        ev1.synchronize()
+        same1 = ev0.elapsed_time(ev1)
+        _, _, tot1 = e1.step_profiled(K_steps, flush_l2=True)
+    fp64_same = st1["dof_per_step"] * K_steps / (same1 * 1e-3)
     fp64_value = st1["dof_per_step"] * K_steps / (tot1 * 1e-3)
+    fp64_state = 30 * ws[0].K * 8
     clocks = sampler.stop()
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K_steps, "warmup": W_steps,
@@ -474,13 +497,22 @@ def run_ours(args):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                         "bytes_per_launch": dom[1], "ms_per_launch": dom[2],
+                         "bytes_per_launch": dom[1], "ms_per_launch": dom[2], "time_source": time_source,
                          "step_GBs": bytes_step / (t_max / K_steps * 1e-3) / 1e9,
                          "kernels": kernels},
             "fp64_plain": {"value": fp64_value, "unit": UNIT, "shots": 1, "K": ws[0].K,
-                           "l2": "flushed before every step", "ms_per_step": tot1 / K_steps,
+                           "kernels": eng.KERNEL_FAMILIES[st1["kernel_family"]],
+                           "l2": "flushed before every step (256 MB write), events around every launch",
+                           "ms_per_step": tot1 / K_steps,
                            "GBs": st1["bytes_per_step"] / (tot1 / K_steps * 1e-3) / 1e9,
-                           "ratio_batched_over_fp64_plain": value / world / fp64_value},
+                           "ratio_batched_over_fp64_plain": value / world / fp64_value,
+                           "value_same_timing": fp64_same,
+                           "same_timing": "one dg_gpu_step(%d) call, CUDA graphs, events around the call, no "
+                                          "flush: the timing of `value`; FP64 state %.0f MB (L2 126 MB)"
+                                          % (K_steps, fp64_state / 1e6),
+                           "ms_per_step_same_timing": same1 / K_steps,
+                           "GBs_same_timing": st1["bytes_per_step"] / (same1 / K_steps * 1e-3) / 1e9,
+                           "ratio_same_timing": value / world / fp64_same},
             "accuracy": accuracy,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "chunk_steps": e2e_chunk,

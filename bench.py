@@ -12,8 +12,11 @@ with host buffers, and the reference's own CPU code timed on this host.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
                     [--precision fp32|fp32_kahan|fp64]
 
-Under torchrun (N > 1) every rank advances its own batch (shots shifted along the surface per
-rank, no collective on the data path); the time is the maximum over ranks.
+Under torchrun (N > 1) the ranks share one job: the multi-shot job has 64 shots per GPU, cut into
+contiguous shot ranges (sharding.shard_shots); the uneven batch's meshes go to ranks by cost
+(sharding.shard_meshes).  Nothing is exchanged while the ranks step; the end-to-end figure ends
+with every rank's traces gathered on rank 0 (sharding.gather_traces).  Times are the maximum over
+ranks.
 """
 from __future__ import annotations
 
@@ -50,31 +53,70 @@ def pkg():
     return importlib.import_module("discontinuous-galerkin-method_b200")
 
 
-def _uneven(steps, rank, n_meshes=48):
-    ws, _ = pkg().workloads.uneven_batch(n_meshes=n_meshes, seed=5 + 97 * rank)
+def _multishot(steps, rank, world):
+    """This rank's share of the multi-shot job: the layered 200,000-triangle mesh with 64 shots per
+    rank (64 * world sources evenly spaced along the surface), cut into contiguous shot ranges by
+    sharding.shard_shots, so every rank advances 64 shots on the wavefront step."""
+    import dataclasses
+    job = pkg().workloads.layered_multishot(steps=steps, shots=64 * world)
+    r = pkg().sharding.shard_shots(job.shots, world)[rank]
+    return [dataclasses.replace(job, src=job.src[r.start:r.stop].copy())]
+
+
+def _uneven(steps, rank, world, n_meshes=48):
+    """This rank's share of the uneven batch: the meshes sharding.shard_meshes gives it by cost
+    (elements x shots x steps)."""
+    ws, _ = pkg().workloads.uneven_batch(n_meshes=n_meshes, seed=5)
     for w in ws:
         w.steps = steps
-    return ws
+    sh = pkg().sharding
+    mine = sh.shard_meshes([sh.mesh_cost(w.K, w.shots, steps) for w in ws], world)[rank]
+    return [ws[i] for i in mine]
+
+
+def _replica(make):
+    """A one-mesh, one-shot workload that does not split: every rank runs the same one."""
+    return lambda steps, rank, world: [make(steps)]
 
 
 WORKLOADS = {
-    # name: (constructor(steps, rank) -> Workload or list of Workloads, description)
-    "multishot": (lambda steps, rank: pkg().workloads.layered_multishot(steps=steps, shot_phase=(rank % 16) / 16.0),
-                  "multi-shot layered elastic batch: 200,000 triangles x 64 shots"),
+    # name: (constructor(steps, rank, world) -> this rank's workloads, description, how N GPUs
+    # share the job: "weak" = a fixed share per GPU, "strong" = a fixed job split, "replicas")
+    "multishot": (_multishot, "multi-shot layered elastic batch: 200,000 triangles x 64 shots per GPU", "weak"),
     # one shot of that mesh: the plain FP64 path's workload, for profiling it on its own
-    "layered1": (lambda steps, rank: one_shot(pkg().workloads.layered_multishot(steps=steps)),
-                 "layered elastic mesh of the multi-shot batch, 200,000 triangles, 1 shot"),
-    "slope": (lambda steps, rank: pkg().workloads.coupled_slope(steps=steps),
-              "coupled acoustic-elastic slope: ~400,000 triangles, 1 shot"),
-    "random": (lambda steps, rank: pkg().workloads.random_medium(steps=steps),
-               "heterogeneous random medium: 2,000,000 triangles, 1 shot"),
-    "square": (lambda steps, rank: pkg().workloads.homogeneous_square(steps=steps),
-               "homogeneous square: 20,000 triangles, 1 shot"),
-    "uneven": (_uneven, "uneven batch: 48 meshes, 5,000-500,000 triangles (log-uniform), 1-8 shots each"),
+    "layered1": (_replica(lambda steps: one_shot(pkg().workloads.layered_multishot(steps=steps))),
+                 "layered elastic mesh of the multi-shot batch, 200,000 triangles, 1 shot", "replicas"),
+    "slope": (_replica(lambda steps: pkg().workloads.coupled_slope(steps=steps)),
+              "coupled acoustic-elastic slope: ~400,000 triangles, 1 shot", "replicas"),
+    "random": (_replica(lambda steps: pkg().workloads.random_medium(steps=steps)),
+               "heterogeneous random medium: 2,000,000 triangles, 1 shot", "replicas"),
+    "square": (_replica(lambda steps: pkg().workloads.homogeneous_square(steps=steps)),
+               "homogeneous square: 20,000 triangles, 1 shot", "replicas"),
+    "uneven": (_uneven, "uneven batch: 48 meshes, 5,000-500,000 triangles (log-uniform), 1-8 shots each, "
+                        "split over the GPUs by cost", "strong"),
     # the first 12 meshes of that batch: a smaller case of the same kernels, for profiling
-    "uneven12": (lambda steps, rank: _uneven(steps, rank, 12),
-                 "uneven batch: 12 meshes, 5,000-500,000 triangles (log-uniform), 1-8 shots each"),
+    "uneven12": (lambda steps, rank, world: _uneven(steps, rank, world, 12),
+                 "uneven batch: 12 meshes, 5,000-500,000 triangles (log-uniform), 1-8 shots each", "strong"),
 }
+
+
+def job_traces(engine, ws, t0, n):
+    """This rank's traces of steps [t0, t0 + n): (shots of all its meshes, 2, n, n_rec) for one
+    mesh, or a flat array of every mesh's block for several (meshes differ in receivers)."""
+    import numpy as np
+    blocks = []
+    for k, _ in enumerate(ws):
+        tx, tz = engine.fetch_traces(t0, n, mesh=k)
+        blocks.append(np.stack([tx, tz], 1))
+    return blocks[0] if len(blocks) == 1 else np.concatenate([b.ravel() for b in blocks])
+
+
+def gather_job(dist, local, device):
+    """Every rank's traces on rank 0 (sharding.gather_traces; the job's one collective), None on
+    the other ranks; a one-rank job returns its own."""
+    if dist is None:
+        return [local]
+    return pkg().sharding.gather_traces(dist, local, root=0, device=device)
 
 
 class ClockSampler:
@@ -167,9 +209,26 @@ def max_over_ranks(x: float, dist, device) -> float:
 
 
 def weak_scaling_value(dof_per_step_per_rank: float, steps: int, local_ms: float, world: int, dist, device):
-    """Whole-job DOF-updates/s: every rank's work over the slowest rank's device time."""
+    """Whole-job DOF-updates/s when every rank does the same work: every rank's work over the
+    slowest rank's device time."""
     t_max = max_over_ranks(local_ms, dist, device)
     return world * dof_per_step_per_rank * steps / (t_max * 1e-3), t_max
+
+
+def sum_over_ranks(x: float, dist, device) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def job_value(dof_per_step_local: float, steps: int, local_ms: float, dist, device):
+    """Whole-job DOF-updates/s for ranks with different shares: all ranks' work over the slowest
+    rank's device time."""
+    t_max = max_over_ranks(local_ms, dist, device)
+    return sum_over_ranks(dof_per_step_local, dist, device) * steps / (t_max * 1e-3), t_max
 
 
 def barrier(dist, device):
@@ -240,8 +299,8 @@ def run_reference_arm(args):
     rank, world, local, dist = dist_setup(args, join=False)
     if rank != 0:
         return 0
-    ctor, desc = WORKLOADS[args.workload]
-    w = as_list(ctor(max(args.steps, args.warmup) + 10, 0))[0]
+    ctor, desc, _ = WORKLOADS[args.workload]
+    w = ctor(max(args.steps, args.warmup) + 10, 0, 1)[0]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refrun
     cores = os.cpu_count() or 1
@@ -313,13 +372,13 @@ def run_ours(args):
     torch.cuda.set_device(device)
     P = pkg()
     eng = P.engine
-    ctor, desc = WORKLOADS[args.workload]
+    ctor, desc, share = WORKLOADS[args.workload]
     K_steps, W_steps = args.steps, args.warmup
     e2e_chunk = 25
     e2e_steps = max(e2e_chunk, (K_steps // e2e_chunk) * e2e_chunk)
     acc_steps = 1000   # FP32 against FP64: long enough for arrivals at the receivers of every workload
     table = max(W_steps + 2 * K_steps, W_steps + e2e_steps, acc_steps) + 8
-    ws = as_list(ctor(table, rank))
+    ws = ctor(table, rank, world)
     setups = [P.host.build_setup(w, full=False, n_steps=table) for w in ws]
     meshes = [eng.mesh_from_setup(s, with_ref_ops=False) for s in setups]
     peak, peak_src = peaks()
@@ -345,7 +404,8 @@ def run_ours(args):
     barrier(dist, device)
     total_ms = ev0.elapsed_time(ev1)
     launches = e.stats()["launches"]
-    value, t_max = weak_scaling_value(dof_step, K_steps, total_ms, world, dist, device)
+    value, t_max = job_value(dof_step, K_steps, total_ms, dist, device)
+    dof_job = sum_over_ranks(dof_step, dist, device)
     names = eng.KERNEL_NAMES[st["kernel_family"]]
     if names[1] is None:
         # the whole step in one launch (or the whole run in one persistent launch): the kernel's
@@ -380,19 +440,27 @@ def run_ours(args):
     wav = torch.empty(len(ws) * e2e_chunk, dtype=torch.float64).pin_memory()
     n_tr = sum(x.shots * x.rec.shape[0] for x in ws) * e2e_chunk
     outs = (torch.empty(n_tr, dtype=torch.float64).pin_memory(), torch.empty(n_tr, dtype=torch.float64).pin_memory())
+    n_chunks = e2e_steps // e2e_chunk
+    kept = np.empty((2, n_chunks, n_tr))  # the run's traces, as a user keeps them
     barrier(dist, device)
     t0 = time.perf_counter()
-    for c in range(e2e_steps // e2e_chunk):
+    for c in range(n_chunks):
         t_at = W_steps + c * e2e_chunk
         for k, s in enumerate(setups):
             wav[k * e2e_chunk:(k + 1) * e2e_chunk].copy_(torch.from_numpy(s.arrays["wavelet"][t_at:t_at + e2e_chunk]))
         e.set_wavelet(t_at, wav, mesh=eng.ALL_MESHES)
         e.step(e2e_chunk)
         e.fetch_traces(t_at, e2e_chunk, mesh=eng.ALL_MESHES, out_x=outs[0], out_z=outs[1])
+        kept[0, c] = outs[0].numpy()
+        kept[1, c] = outs[1].numpy()
+    # the job's one collective: every rank's traces to rank 0
+    gathered = gather_job(dist, kept, device)
     t_e2e = time.perf_counter() - t0
     barrier(dist, device)
     t_e2e = max_over_ranks(t_e2e, dist, device)
-    e2e_value = world * dof_step * e2e_steps / t_e2e
+    e2e_value = dof_job * e2e_steps / t_e2e
+    if rank == 0:
+        assert len(gathered) == world and all(np.isfinite(g).all() for g in gathered)
     h2d = 8.0 * len(ws)
     d2h = 2.0 * 8.0 * R_tot
 
@@ -485,12 +553,18 @@ def run_ours(args):
     clocks = sampler.stop()
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K_steps, "warmup": W_steps,
-            "ms_per_step": t_max / K_steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": t_max / K_steps, "higher_is_better": True,
+            "scaling": {"weak": "weak", "strong": "strong", "replicas": "weak"}[share], "vs_baseline": None,
             "dtype": {"fp32": "f32", "fp32_kahan": "f32 (Kahan-compensated)", "fp64": "f64"}[args.precision],
             "data": "synthetic (seeded meshes and media)",
             "config": {"workload": desc, "meshes": len(ws), "K": K_tot, "shots": S_tot, "precision": args.precision,
                        "kernels": eng.KERNEL_FAMILIES[st["kernel_family"]],
-                       "parallelism": "independent batches per GPU" if world > 1 else "single GPU",
+                       "parallelism": ("single GPU" if world == 1 else
+                                       {"weak": "one job of %d shots, 64 contiguous shots per GPU (shard_shots)"
+                                                % (64 * world),
+                                        "strong": "one job of meshes split over %d GPUs by cost (shard_meshes)"
+                                                  % world,
+                                        "replicas": "the same one-shot mesh on every GPU (no split)"}[share]),
                        "l2": ("inputs larger than L2: state %.2f GB per GPU" % (state_bytes / 1e9))
                        if state_bytes > 126e6 * 1.5 else "state smaller than L2 (not flushed)",
                        "block_threads": st["block_threads"]},
@@ -518,7 +592,8 @@ def run_ours(args):
                     "chunk_steps": e2e_chunk,
                     "what": "dg_gpu_set_wavelet (every mesh, pinned host wavelets) + dg_gpu_step + "
                             "dg_gpu_fetch_traces (every mesh and shot, pinned host buffers) per %d-step chunk, "
-                            "wall clock" % e2e_chunk},
+                            "then every rank's traces gathered on rank 0 (sharding.gather_traces), wall clock, "
+                            "slowest rank" % e2e_chunk},
             "clocks": clocks}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(ws[0])

@@ -44,6 +44,8 @@ def lib():
         _LIB.dgo_max_threads.restype = C.c_int
         _LIB.dgo_half.restype = C.c_int
         _LIB.dgo_half.argtypes = [C.c_void_p, C.c_long, C.c_long, C.c_int] + [C.c_void_p] * 7
+        _LIB.dgo_set_flush_subnormals.argtypes = [C.c_int]
+        _LIB.dgo_set_flush_subnormals.restype = None
     return _LIB
 
 
@@ -74,14 +76,21 @@ class Oracle:
         self.fields = [np.zeros(self.K * 6) for _ in range(5)]
         self.t = 0
 
-    def run(self, shot: int, steps: int, threads: int = 0, record: bool = True):
+    def run(self, shot: int, steps: int, threads: int = 0, record: bool = True, flush_subnormals: bool = False):
+        """`steps` steps of `shot`; with flush_subnormals the loops flush subnormal values to zero
+        (for long runs compared at a relative tolerance only: values below 2^-1022 become 0)."""
         if self.fields is None:
             self.reset()
         rx = np.zeros((steps, self.n_rec)) if record else None
         rz = np.zeros((steps, self.n_rec)) if record else None
         f = self.fields
-        rc = lib().dgo_run(C.byref(self.prob), shot, self.t, steps, *(a.ctypes.data for a in f),
-                           None if rx is None else rx.ctypes.data, None if rz is None else rz.ctypes.data, threads)
+        lib().dgo_set_flush_subnormals(1 if flush_subnormals else 0)
+        try:
+            rc = lib().dgo_run(C.byref(self.prob), shot, self.t, steps, *(a.ctypes.data for a in f),
+                               None if rx is None else rx.ctypes.data, None if rz is None else rz.ctypes.data,
+                               threads)
+        finally:
+            lib().dgo_set_flush_subnormals(0)
         if rc != 0:
             raise RuntimeError("oracle run failed (%d)" % rc)
         self.t += steps

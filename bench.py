@@ -386,7 +386,7 @@ def run_ours(args):
     sampler.start()
 
     # ---- headline: the batch in the requested arithmetic, inputs resident in HBM ------------
-    e = eng.Engine(meshes, args.precision, device=device)
+    e = eng.Engine(meshes, args.precision, device=device, variant=args.variant)
     st = e.stats()
     bytes_step, dof_step = st["bytes_per_step"], st["dof_per_step"]
     e.step(W_steps)
@@ -558,7 +558,7 @@ def run_ours(args):
             "dtype": {"fp32": "f32", "fp32_kahan": "f32 (Kahan-compensated)", "fp64": "f64"}[args.precision],
             "data": "synthetic (seeded meshes and media)",
             "config": {"workload": desc, "meshes": len(ws), "K": K_tot, "shots": S_tot, "precision": args.precision,
-                       "kernels": eng.KERNEL_FAMILIES[st["kernel_family"]],
+                       "kernels": eng.KERNEL_FAMILIES[st["kernel_family"]], "variant": args.variant,
                        "parallelism": ("single GPU" if world == 1 else
                                        {"weak": "one job of %d shots, 64 contiguous shots per GPU (shard_shots)"
                                                 % (64 * world),
@@ -614,6 +614,9 @@ def main(argv=None):
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="multishot")
     ap.add_argument("--precision", choices=["fp32", "fp32_kahan", "fp64"], default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="dg_gpu_opts.variant of the headline run (0 automatic; 4: odd shot counts without "
+                         "the padding shot)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

@@ -97,7 +97,7 @@ def test_reference_arm_is_rank0_only(monkeypatch):
     monkeypatch.setenv("RANK", "1")
     monkeypatch.setenv("LOCAL_RANK", "1")
     args = bench.argparse.Namespace(gpus=2, steps=1, warmup=3, impl="reference", workload="square",
-                                    no_cpu_baseline=False)
+                                    no_cpu_baseline=False, variant=0)
     assert bench.run_reference_arm(args) == 0     # returns before any work on a non-zero rank
     import torch.distributed as dist
     assert not dist.is_initialized()              # and joins no process group

@@ -615,8 +615,7 @@ def main(argv=None):
     ap.add_argument("--precision", choices=["fp32", "fp32_kahan", "fp64"], default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=0,
-                    help="dg_gpu_opts.variant of the headline run (0 automatic; 4: odd shot counts without "
-                         "the padding shot)")
+                    help="dg_gpu_opts.variant of the headline run (0 automatic; see include/dg_gpu.h)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

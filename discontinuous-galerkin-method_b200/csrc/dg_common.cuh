@@ -90,9 +90,7 @@ template <class R> struct MeshDev {
                           // blocks [block0, n_elem_blocks) and then the recorder blocks (a window
                           // of a split mesh's half step; 0 otherwise)
   int kind;               // FP32 kernel body: 0 one (element, shot) per thread, plane-major;
-                          // 1 two elements per thread (S = 1); 2 two shots per thread, element-major;
-                          // 3 the same, plane-major; 4 the same, plane-major, an odd shot count
-                          // stored without the padding shot (ES shots stored, S = ES + 1 lanes' worth)
+                          // 1 two elements per thread (S = 1); 2 two shots per thread, element-major
   int sponge_elems;
   R dt;
   R* U;                   // [30][P]
@@ -169,14 +167,9 @@ __device__ __forceinline__ void record(const MeshDev<R>& m, int lb_rec, long lon
   const int S = m.S;
   if (q >= m.n_rec * S) return;
   const int r = q / S, s = q - r * S;
-  R* tr = m.trace + (t * 2) * (long long)m.n_rec * S;
-  if (m.kind == 4 && s >= m.ES) {  // the padding slot of an odd count stored without it
-    tr[q] = R(0);
-    tr[(long long)m.n_rec * S + q] = R(0);
-    return;
-  }
   const int e = __ldg(m.rec_elem + r), node = __ldg(m.rec_node + r);
   const long long at = (long long)e * m.ES + s;
+  R* tr = m.trace + (t * 2) * (long long)m.n_rec * S;
   tr[q] = m.U[at + (0 + node) * m.PS];
   tr[(long long)m.n_rec * S + q] = m.U[at + (6 + node) * m.PS];
 }

@@ -77,8 +77,7 @@ void set_last_error(const char* msg) { g_last = msg ? msg : ""; }
 struct MeshHostInfo {
   long K = 0;
   int Kp = 0, S = 0, n_rec = 0;
-  int S_pad = 0;  // shots computed (S plus a silent shot where the packed kernels need an even count)
-  int S_store = 0;  // shots stored per element and plane (S_pad, or S on the unpadded odd layout)
+  int S_pad = 0;  // shots stored (S plus a silent shot where the packed kernels need an even count)
   int kind = 0;   // kernel body (MeshDev::kind)
   long steps = 0;
   std::vector<int> new_of_old;  // caller element -> internal element
@@ -226,8 +225,7 @@ constexpr long long P2_IBE[9] = {6, 4, 1, 1, 2, 3, 6, 5, 3};
 struct Prepared {
   long K;
   int Kp, S, n_rec;
-  int S_pad = 0;  // shots computed (S, or S + 1 silent shot for the packed kernels)
-  int S_store = 0;  // shots stored per element and plane (S_pad, or S on the unpadded odd layout)
+  int S_pad = 0;  // shots stored and computed (S, or S + 1 silent shot for the packed kernels)
   int kind = 0;   // kernel body, as MeshDev::kind
   std::vector<int> order;       // internal -> caller element
   std::vector<int> new_of_old;  // caller -> internal
@@ -557,12 +555,12 @@ int upload_mesh(dg_gpu_ctx* c, const dg_gpu_mesh& m, Prepared& p, MeshDev<R>& d)
   d.S = p.S_pad;
   d.n_rec = p.n_rec;
   d.kind = p.kind;
-  d.P = (long long)p.Kp * p.S_store;
+  d.P = (long long)p.Kp * p.S_pad;
   if (p.kind == 2) {  // element-major: U[e][plane][S]
     d.ES = 30LL * p.S_pad;
     d.PS = p.S_pad;
-  } else {            // plane-major: U[plane][e*S + s], S = the stored shots
-    d.ES = p.S_store;
+  } else {            // plane-major: U[plane][e*S + s]
+    d.ES = p.S_pad;
     d.PS = d.P;
   }
   d.steps = m.n_steps;
@@ -837,10 +835,9 @@ bool x2pm_supported(int S) { return S >= 2 && S <= 16 && S % 2 == 0; }
 // layout up to 14 stored shots, element-major above or for the wavefront step), an odd count
 // padded with one silent shot — unless the caller asks for one (element, shot) per thread
 // (variant 1).
-void choose_kind(int S, long K, bool fp32, int variant, bool want_wave, int& kind, int& S_pad, int& S_store) {
+void choose_kind(int S, long K, bool fp32, int variant, bool want_wave, int& kind, int& S_pad) {
   kind = 0;
   S_pad = S;
-  S_store = S;
   if (!fp32 || variant == 1) return;
   if (S == 1) {
     kind = 1;
@@ -854,20 +851,9 @@ void choose_kind(int S, long K, bool fp32, int variant, bool want_wave, int& kin
     // gives each thread a whole element record, 163 G, below one (element, shot) per thread,
     // 248 G, while the plane-major body runs at 319 G, and 405 G against 276 G on 2M elements);
     // the wavefront step needs the element-major layout
-    const bool pm = x2pm_supported(even) &&
-                    (variant == 3 || (variant == 4 && (S & 1) && S <= 13) || (variant == 0 && !want_wave && even <= 14));
+    const bool pm = x2pm_supported(even) && (variant == 3 || (variant == 0 && !want_wave && even <= 14));
     kind = pm ? 3 : 2;
     S_pad = even;
-    S_store = even;
-    // on request (variant 4) an odd count on the plane-major layout is stored without its padding
-    // shot (kind 4): the element's last lane reads and writes one value per plane instead of two,
-    // so the silent shot moves no memory; it is not the default because the lanes then load
-    // scalars, twice the load instructions: the 48-mesh uneven batch runs at 347 G DOF-updates/s
-    // that way against 370 G padded
-    if (variant == 4 && (S & 1) && S <= 13) {
-      kind = 4;
-      S_store = S;
-    }
   }
 }
 
@@ -1076,7 +1062,7 @@ int zero_state(dg_gpu_ctx* c) {
     void* U = c->is_double ? (void*)c->md_d[k].U : (void*)c->md_f[k].U;
     void* C = c->is_double ? (void*)c->md_d[k].C : (void*)c->md_f[k].C;
     void* T = c->is_double ? (void*)c->md_d[k].trace : (void*)c->md_f[k].trace;
-    const size_t P = (size_t)h.Kp * h.S_store;
+    const size_t P = (size_t)h.Kp * h.S_pad;
     CK(cudaMemsetAsync(U, 0, esz * NPLANES * P, c->stream));
     if (C) CK(cudaMemsetAsync(C, 0, esz * NPLANES * P, c->stream));
     CK(cudaMemsetAsync(T, 0, esz * (size_t)h.steps * 2 * std::max(1, h.n_rec) * h.S_pad, c->stream));
@@ -1251,7 +1237,7 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   for (int k = 0; k < n_meshes; k++) {
     Prepared p;
     choose_kind(meshes[k].n_shots, meshes[k].K, !c->is_double, variant, o.wavefront == 1 && n_meshes == 1, p.kind,
-                p.S_pad, p.S_store);
+                p.S_pad);
     if (o.variant == 2 && p.kind == 0)
       return fail(DG_ERR_UNSUPPORTED, "no packed FP32 kernel for this mesh (FP32 only; at most 128 shots)");
     // the wavefront step: one FP32 mesh on the two-shot kernels; automatic = on
@@ -1278,11 +1264,10 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
     h.Kp = p.Kp;
     h.S = p.S;
     h.S_pad = p.S_pad;
-    h.S_store = p.S_store;
     h.kind = p.kind;
     if (!c->multi) {
-      c->x2 = p.kind == 1 ? 1 : (p.kind == 4 ? p.S_store : (p.kind >= 2 ? p.S_pad : 0));
-      c->x2pm = p.kind == 3 || p.kind == 4;
+      c->x2 = p.kind == 1 ? 1 : (p.kind >= 2 ? p.S_pad : 0);
+      c->x2pm = p.kind == 3;
     }
     if (c->wave) {
       c->face_h = p.face;
@@ -1414,7 +1399,7 @@ static int enqueue_steps(dg_gpu_ctx* c, long n, bool timed) {
     if (c->watchdog_every > 0 && c->t % c->watchdog_every == 0) {
       CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
       for (size_t k = 0; k < c->mi.size(); k++) {
-        const long long nvals = 30LL * c->mi[k].Kp * c->mi[k].S_store;
+        const long long nvals = 30LL * c->mi[k].Kp * c->mi[k].S_pad;
         if (c->is_double) k_nonfinite<double><<<592, 256, 0, c->stream>>>(c->md_d[k].U, nvals, c->d_flag);
         else k_nonfinite<float><<<592, 256, 0, c->stream>>>(c->md_f[k].U, nvals, c->d_flag);
         c->stats.launches++;

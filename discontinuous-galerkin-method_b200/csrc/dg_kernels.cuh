@@ -37,14 +37,14 @@ MxpFn kernel_batch_persistent(bool kahan);                        // dg_k_multi.
 
 // the packed instances, split by shot count over three translation units
 HalfPair<X2Fn> kernels_packed_small(int S, bool kahan, bool pm);  // S = 2..8
-HalfPair<X2Fn> kernels_packed_mid(int S, bool kahan, bool pm);    // S = 9..16
+HalfPair<X2Fn> kernels_packed_mid(int S, bool kahan, bool pm);    // S = 10..16
 HalfPair<X2Fn> kernels_packed_large(int S, bool kahan);           // S = 1, 32, 64, 128
 
-// S stored shots (even: element-major, or plane-major with `pm`; odd up to 13: plane-major
-// without a padding shot), or S = 1: two elements per thread on the one-shot plane-major layout
+// S stored shots (even; element-major, or plane-major with `pm`), or S = 1: two elements per
+// thread on the one-shot plane-major layout
 inline HalfPair<X2Fn> kernels_packed(int S, bool kahan, bool pm) {
   if (S >= 2 && S <= 8) return kernels_packed_small(S, kahan, pm);
-  if (S >= 9 && S <= 16) return kernels_packed_mid(S, kahan, pm);
+  if (S >= 10 && S <= 16) return kernels_packed_mid(S, kahan, pm);
   if (pm) return {};
   return kernels_packed_large(S, kahan);
 }

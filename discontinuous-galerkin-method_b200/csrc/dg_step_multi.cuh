@@ -1,10 +1,9 @@
 // dg_step_multi.cuh — one launch per half-step over a batch of FP32 meshes with their own shot
 // counts, time steps and step counts.  Each block belongs to one mesh (block table) and runs the
 // kernel body that suits that mesh: two elements per thread for one shot, two shots per thread
-// (packed FP32x2) for even shot counts on element-major (kind 2) or plane-major (kind 3) state and
-// for odd counts above one on plane-major state stored without a padding shot (kind 4; the
-// padded element-major form of odd counts remains for larger ones), and one (element, shot) per
-// thread otherwise.
+// (packed FP32x2, element-major layout) for even shot counts — odd counts above one are padded
+// on the host with one silent shot, on element-major or (kind 3) plane-major state — and one
+// (element, shot) per thread otherwise.
 #pragma once
 #include "dg_common.cuh"
 #include "dg_step_generic.cuh"
@@ -15,7 +14,6 @@ namespace dg {
 #define DG_MX_SHOTS(CALL) \
   CALL(2) CALL(4) CALL(6) CALL(8) CALL(10) CALL(12) CALL(14) CALL(16) CALL(32) CALL(64) CALL(128)
 #define DG_MX_PM_SHOTS(CALL) CALL(2) CALL(4) CALL(6) CALL(8) CALL(10) CALL(12) CALL(14) CALL(16)
-#define DG_MX_ODD_SHOTS(CALL) CALL(3) CALL(5) CALL(7) CALL(9) CALL(11) CALL(13)
 
 // The velocity half of one block of the batch: block lb of mesh m, in the body of its kind.
 template <bool KAHAN>
@@ -42,12 +40,6 @@ __device__ __forceinline__ void mx_velocity_block(const Ops<float>& ops, const O
     velocity_x2_body<SS, KAHAN, true>(ops2, m, lb, t); \
     break;
       DG_MX_PM_SHOTS(DG_MX_VP)
-      default:
-        break;
-    }
-  } else if (m.kind == 4) {
-    switch ((int)m.ES) {  // the stored (odd) shot count
-      DG_MX_ODD_SHOTS(DG_MX_VP)
 #undef DG_MX_VP
       default:
         break;
@@ -86,12 +78,6 @@ __device__ __forceinline__ void mx_stress_block(const Ops<float>& ops, const Ops
     stress_x2_body<SS, KAHAN, false, true>(ops2, m, lb, t); \
     break;
       DG_MX_PM_SHOTS(DG_MX_TP)
-      default:
-        break;
-    }
-  } else if (m.kind == 4) {
-    switch ((int)m.ES) {
-      DG_MX_ODD_SHOTS(DG_MX_TP)
 #undef DG_MX_TP
       default:
         break;

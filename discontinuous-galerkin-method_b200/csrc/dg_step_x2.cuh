@@ -42,66 +42,27 @@ __device__ __forceinline__ void kahan2(float2& u, float2& c, float2 d) {
   u = t;
 }
 
-// Load of a velocity value: plain, or through L2 (FRESH) when other blocks of the same launch
-// wrote it (the wavefront step), so no stale L1 line can be returned.
-template <bool FRESH>
-__device__ __forceinline__ float2 ld_v(const float2* p) {
-  if (FRESH) return __ldcg(p);
-  return *p;
-}
-template <bool FRESH>
-__device__ __forceinline__ float ld_v1(const float* p) {
-  if (FRESH) return __ldcg(p);
-  return *p;
-}
-
-// A lane's two shots of one plane of one element, at p: one float2 for an even stored shot
-// count; for an odd count, stored without a padding shot (plane-major only), the float at p and
-// the next one, which the element's last lane does not have (has_y false: it reads and writes
-// only the first, and computes on a zero in place of the second).
-template <int S, bool FRESH = false>
-__device__ __forceinline__ float2 ldp(const float* p, bool has_y) {
-  if constexpr ((S & 1) == 0) {
-    return ld_v<FRESH>(reinterpret_cast<const float2*>(p));
-  } else {
-    const float x = ld_v1<FRESH>(p);
-    return make_float2(x, has_y ? ld_v1<FRESH>(p + 1) : 0.f);
-  }
-}
-template <int S>
-__device__ __forceinline__ void stp(float* p, float2 v, bool has_y) {
-  if constexpr ((S & 1) == 0) {
-    *reinterpret_cast<float2*>(p) = v;
-  } else {
-    p[0] = v.x;
-    if (has_y) p[1] = v.y;
-  }
-}
-
 // Bodies take the mesh, the block's index within that mesh and the step; the __global__
 // wrappers below (one mesh) and the multi-mesh dispatchers (dg_step_multi.cuh) call them.
-// PM: plane-major layout U[plane][e*S + s] (plane stride Kp*S floats) instead of the
-// element-major U[e][plane][S]; the arithmetic is the same.  S is the stored shot count: even,
-// or odd on the plane-major layout (no padding shot stored: see ldp).  Lane q of an element
-// advances shots 2q and 2q+1; (S + 1) / 2 lanes per element.
+// PM: plane-major layout U[plane][e*S + s] (plane stride Kp*S/2 float2) instead of the
+// element-major U[e][plane][S]; the arithmetic is the same.
 template <int S, bool KAHAN, bool PM = false>
 __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
-  static_assert((S & 1) == 0 || PM, "odd stored shot counts are plane-major");
-  constexpr int H = (S + 1) / 2;                          // lanes per element
-  const long long EO = PM ? S : 30LL * S;                 // element offset, floats
-  const long long PS = PM ? (long long)m.Kp * S : S;      // plane stride, floats
+  constexpr int H = S / 2;    // float2 lanes per element
+  constexpr int ES = 30 * H;  // element stride in float2 (element-major)
+  const long long EO = PM ? H : ES;                   // element offset
+  const long long PS = PM ? (long long)m.Kp * H : H;  // plane stride
   const int g = lb * blockDim.x + threadIdx.x;
   if (g >= m.K * H) return;
   const int e = g / H, q = g - e * H;
-  const bool has_y = (S & 1) == 0 || 2 * q + 1 < S;
-  float* __restrict__ Ue = m.U + (long long)e * EO + 2 * q;
+  float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * EO + q;
 
   float2 txx[NP], tzz[NP], txz[NP];
 #pragma unroll
   for (int i = 0; i < NP; i++) {
-    txx[i] = ldp<S>(Ue + (12 + i) * PS, has_y);
-    tzz[i] = ldp<S>(Ue + (18 + i) * PS, has_y);
-    txz[i] = ldp<S>(Ue + (24 + i) * PS, has_y);
+    txx[i] = Ue[(12 + i) * PS];
+    tzz[i] = Ue[(18 + i) * PS];
+    txz[i] = Ue[(24 + i) * PS];
   }
   const int4 fc = __ldg(m.face + e);
   const float4 gm = __ldg(m.geo + e);
@@ -134,13 +95,13 @@ __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<
       for (int k = 0; k < NF; k++) { pxx[k] = f2(0.f); pzz[k] = f2(0.f); pxz[k] = f2(0.f); }
     } else {
       const int nb = code >> 4, nf = (code >> 1) & 3, flip = code & 1;
-      const float* __restrict__ Un = m.U + (long long)nb * EO + 2 * q;
+      const float2* __restrict__ Un = reinterpret_cast<const float2*>(m.U) + (long long)nb * EO + q;
 #pragma unroll
       for (int k = 0; k < NF; k++) {
         const int node = face_node(nf, flip ? 2 - k : k);
-        pxx[k] = ldp<S>(Un + (12 + node) * PS, has_y);
-        pzz[k] = ldp<S>(Un + (18 + node) * PS, has_y);
-        pxz[k] = ldp<S>(Un + (24 + node) * PS, has_y);
+        pxx[k] = Un[(12 + node) * PS];
+        pzz[k] = Un[(18 + node) * PS];
+        pxz[k] = Un[(24 + node) * PS];
       }
       if (code & 8) {
 #pragma unroll
@@ -196,12 +157,12 @@ __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<
   // V = a V (+ source on Vz) + dt/rho * rhs
   float2 vx[NP], vz[NP], cx[NP], cz[NP];
 #pragma unroll
-  for (int i = 0; i < NP; i++) { vx[i] = ldp<S>(Ue + (0 + i) * PS, has_y); vz[i] = ldp<S>(Ue + (6 + i) * PS, has_y); }
-  float* __restrict__ Ce = nullptr;
+  for (int i = 0; i < NP; i++) { vx[i] = Ue[(0 + i) * PS]; vz[i] = Ue[(6 + i) * PS]; }
+  float2* __restrict__ Ce = nullptr;
   if (KAHAN) {
-    Ce = m.C + (long long)e * EO + 2 * q;
+    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * EO + q;
 #pragma unroll
-    for (int i = 0; i < NP; i++) { cx[i] = ldp<S>(Ce + (0 + i) * PS, has_y); cz[i] = ldp<S>(Ce + (6 + i) * PS, has_y); }
+    for (int i = 0; i < NP; i++) { cx[i] = Ce[(0 + i) * PS]; cz[i] = Ce[(6 + i) * PS]; }
   }
   if (own_sponge) {
 #pragma unroll
@@ -233,12 +194,12 @@ __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<
       vx[i] = fma2(step, hx[i], vx[i]);
       vz[i] = fma2(step, hz[i], add2(vz[i], src[i]));
     }
-    stp<S>(Ue + (0 + i) * PS, vx[i], has_y);
-    stp<S>(Ue + (6 + i) * PS, vz[i], has_y);
+    Ue[(0 + i) * PS] = vx[i];
+    Ue[(6 + i) * PS] = vz[i];
   }
   if (KAHAN) {
 #pragma unroll
-    for (int i = 0; i < NP; i++) { stp<S>(Ce + (0 + i) * PS, cx[i], has_y); stp<S>(Ce + (6 + i) * PS, cz[i], has_y); }
+    for (int i = 0; i < NP; i++) { Ce[(0 + i) * PS] = cx[i]; Ce[(6 + i) * PS] = cz[i]; }
   }
 }
 
@@ -251,6 +212,14 @@ __global__ void __launch_bounds__(256, 2) k_velocity_x2(const __grid_constant__ 
   if (threadIdx.x == 0 && blockIdx.x == 0) ctr->s = t;
   if (t >= m.steps) return;
   velocity_x2_body<S, KAHAN, PM>(ops, m, blockIdx.x + m.block0, t);
+}
+
+// Load of a velocity value: plain, or through L2 (FRESH) when other blocks of the same launch
+// wrote it (the wavefront step), so no stale L1 line can be returned.
+template <bool FRESH>
+__device__ __forceinline__ float2 ld_v(const float2* p) {
+  if (FRESH) return __ldcg(p);
+  return *p;
 }
 
 // The per-element constants of the stress update: face codes, geometric factors, materials.
@@ -266,18 +235,15 @@ __device__ __forceinline__ StressConst stress_const(const MeshDev<float>& m, int
 template <int S, bool KAHAN, bool FRESH, bool PM = false>
 __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<float>& m, int e, int q,
                                                const StressConst& k) {
-  static_assert((S & 1) == 0 || PM, "odd stored shot counts are plane-major");
-  const long long EO = PM ? S : 30LL * S;                 // element offset, floats
-  const long long PS = PM ? (long long)m.Kp * S : S;      // plane stride, floats
-  const bool has_y = (S & 1) == 0 || 2 * q + 1 < S;
-  float* __restrict__ Ue = m.U + (long long)e * EO + 2 * q;
+  constexpr int H = S / 2;
+  constexpr int ES = 30 * H;
+  const long long EO = PM ? H : ES;                   // element offset
+  const long long PS = PM ? (long long)m.Kp * H : H;  // plane stride
+  float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * EO + q;
 
   float2 vx[NP], vz[NP];
 #pragma unroll
-  for (int i = 0; i < NP; i++) {
-    vx[i] = ldp<S, FRESH>(Ue + (0 + i) * PS, has_y);
-    vz[i] = ldp<S, FRESH>(Ue + (6 + i) * PS, has_y);
-  }
+  for (int i = 0; i < NP; i++) { vx[i] = ld_v<FRESH>(Ue + (0 + i) * PS); vz[i] = ld_v<FRESH>(Ue + (6 + i) * PS); }
   const int4 fc = k.fc;
   const float4 gm = k.gm;
   const float4 mt = k.mt;
@@ -315,12 +281,12 @@ __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<fl
       for (int k = 0; k < NF; k++) { px[k] = f2(0.f); pz[k] = f2(0.f); }
     } else {
       const int nb = code >> 4, nf = (code >> 1) & 3, flip = code & 1;
-      const float* __restrict__ Un = m.U + (long long)nb * EO + 2 * q;
+      const float2* __restrict__ Un = reinterpret_cast<const float2*>(m.U) + (long long)nb * EO + q;
 #pragma unroll
       for (int k = 0; k < NF; k++) {
         const int node = face_node(nf, flip ? 2 - k : k);
-        px[k] = ldp<S, FRESH>(Un + (0 + node) * PS, has_y);
-        pz[k] = ldp<S, FRESH>(Un + (6 + node) * PS, has_y);
+        px[k] = ld_v<FRESH>(Un + (0 + node) * PS);
+        pz[k] = ld_v<FRESH>(Un + (6 + node) * PS);
       }
     }
     float2 fa[NF], fb[NF], fw[NF];
@@ -347,19 +313,15 @@ __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<fl
   float2 txx[NP], tzz[NP], txz[NP], cxx[NP], czz[NP], cxz[NP];
 #pragma unroll
   for (int i = 0; i < NP; i++) {
-    txx[i] = ldp<S>(Ue + (12 + i) * PS, has_y);
-    tzz[i] = ldp<S>(Ue + (18 + i) * PS, has_y);
-    txz[i] = ldp<S>(Ue + (24 + i) * PS, has_y);
+    txx[i] = Ue[(12 + i) * PS];
+    tzz[i] = Ue[(18 + i) * PS];
+    txz[i] = Ue[(24 + i) * PS];
   }
-  float* __restrict__ Ce = nullptr;
+  float2* __restrict__ Ce = nullptr;
   if (KAHAN) {
-    Ce = m.C + (long long)e * EO + 2 * q;
+    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * EO + q;
 #pragma unroll
-    for (int i = 0; i < NP; i++) {
-      cxx[i] = ldp<S>(Ce + (12 + i) * PS, has_y);
-      czz[i] = ldp<S>(Ce + (18 + i) * PS, has_y);
-      cxz[i] = ldp<S>(Ce + (24 + i) * PS, has_y);
-    }
+    for (int i = 0; i < NP; i++) { cxx[i] = Ce[(12 + i) * PS]; czz[i] = Ce[(18 + i) * PS]; cxz[i] = Ce[(24 + i) * PS]; }
   }
   if (fc.w & 1) {
 #pragma unroll
@@ -384,23 +346,21 @@ __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<fl
       tzz[i] = add2(tzz[i], dzz);
       txz[i] = add2(txz[i], dxz);
     }
-    stp<S>(Ue + (12 + i) * PS, txx[i], has_y);
-    stp<S>(Ue + (18 + i) * PS, tzz[i], has_y);
-    stp<S>(Ue + (24 + i) * PS, txz[i], has_y);
+    Ue[(12 + i) * PS] = txx[i];
+    Ue[(18 + i) * PS] = tzz[i];
+    Ue[(24 + i) * PS] = txz[i];
   }
   if (KAHAN) {
 #pragma unroll
     for (int i = 0; i < NP; i++) {
-      stp<S>(Ce + (12 + i) * PS, cxx[i], has_y);
-      stp<S>(Ce + (18 + i) * PS, czz[i], has_y);
-      stp<S>(Ce + (24 + i) * PS, cxz[i], has_y);
+      Ce[(12 + i) * PS] = cxx[i]; Ce[(18 + i) * PS] = czz[i]; Ce[(24 + i) * PS] = cxz[i];
     }
   }
 }
 
 template <int S, bool KAHAN, bool FRESH = false, bool PM = false>
 __device__ __forceinline__ void stress_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
-  constexpr int H = (S + 1) / 2;
+  constexpr int H = S / 2;
   const int g = lb * blockDim.x + threadIdx.x;
   if (g >= m.K * H) return;
   const int e = g / H, q = g - e * H;

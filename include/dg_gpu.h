@@ -100,10 +100,7 @@ typedef struct {
 	const char *tune_cache; /* file that keeps autotune results between runs (NULL: none) */
 	int variant;         /* FP32 kernels: 0 automatic, 1 one (element, shot) per thread,
 	                        2 packed FP32x2 kernels (two elements or two shots per thread; element-major
-	                        state for two shots per thread), 3 the same with plane-major state for 2-16 shots,
-	                        4 as 0, except that a mesh of 3, 5, ..., 13 shots is stored plane-major without the
-	                        padding shot the packed kernels otherwise add (less memory traffic, more load
-	                        instructions: slower on the benchmark batches, so not the default) */
+	                        state for two shots per thread), 3 the same with plane-major state for 2-16 shots */
 	int wavefront;       /* one launch per step that keeps the state in flight in L2 (single FP32 mesh
 	                        of 1, 2, 4, ..., 128 shots): 0 automatic (on from 16 shots), 1 on, -1 off */
 } dg_gpu_opts;

@@ -448,31 +448,6 @@ def test_poly_model_against_oracle():
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp32_kahan"])
-def test_odd_shots_without_padding_equal_padded(precision):
-    """variant 4 stores meshes of 3, 5 and 7 shots plane-major without the padding shot the packed
-    kernels otherwise add: the same values bit for bit as the padded layout (each shot's arithmetic
-    is unchanged), for one mesh and for a batch of meshes in one launch."""
-    g = Golden("square_3shots")
-    a = g.setup_arrays()
-    m3 = eng.mesh_from_setup(a)
-    m5, _ = _repeat_shots(a, 5)
-    m7, _ = _repeat_shots(a, 7)
-    for meshes in ([m3], [m5], [m3, m5, m7]):
-        out = []
-        for variant in (0, 4):
-            with eng.Engine(meshes, precision, variant=variant) as e:
-                if len(meshes) == 1:
-                    assert e.stats()["kernel_family"] == 7
-                e.step(g.steps)
-                shots = [np.asarray(mm["source"]).size // 2 for mm in meshes]
-                out.append([e.fetch(f, k, s) for k, S in enumerate(shots) for s in range(S) for f in FIELDS] +
-                           [e.fetch("trace_z", k, s) for k, S in enumerate(shots) for s in range(S)])
-        for x, y in zip(*out):
-            assert np.abs(x).max() > 0
-            assert np.array_equal(x, y)
-
-
-@pytest.mark.parametrize("precision", ["fp32", "fp32_kahan"])
 def test_whole_run_in_one_graph(precision):
     """graph_steps equal to the run's steps puts the whole run in one captured graph (the 64-shot
     configuration's "4,000 steps as one CUDA graph"): the same bits as the default 100-step graphs,

@@ -439,9 +439,10 @@ def run_ours(args):
     # every mesh's wavelet chunk in one pinned buffer and one call, every mesh's traces in one call
     wav = torch.empty(len(ws) * e2e_chunk, dtype=torch.float64).pin_memory()
     n_tr = sum(x.shots * x.rec.shape[0] for x in ws) * e2e_chunk
-    outs = (torch.empty(n_tr, dtype=torch.float64).pin_memory(), torch.empty(n_tr, dtype=torch.float64).pin_memory())
     n_chunks = e2e_steps // e2e_chunk
-    kept = np.empty((2, n_chunks, n_tr))  # the run's traces, as a user keeps them
+    # the run's traces, as a user keeps them: each chunk's fetch lands in its own slice of one
+    # pinned buffer
+    kept = torch.empty((2, n_chunks, n_tr), dtype=torch.float64).pin_memory()
     barrier(dist, device)
     t0 = time.perf_counter()
     for c in range(n_chunks):
@@ -450,11 +451,9 @@ def run_ours(args):
             wav[k * e2e_chunk:(k + 1) * e2e_chunk].copy_(torch.from_numpy(s.arrays["wavelet"][t_at:t_at + e2e_chunk]))
         e.set_wavelet(t_at, wav, mesh=eng.ALL_MESHES)
         e.step(e2e_chunk)
-        e.fetch_traces(t_at, e2e_chunk, mesh=eng.ALL_MESHES, out_x=outs[0], out_z=outs[1])
-        kept[0, c] = outs[0].numpy()
-        kept[1, c] = outs[1].numpy()
+        e.fetch_traces(t_at, e2e_chunk, mesh=eng.ALL_MESHES, out_x=kept[0, c], out_z=kept[1, c])
     # the job's one collective: every rank's traces to rank 0
-    gathered = gather_job(dist, kept, device)
+    gathered = gather_job(dist, kept.numpy(), device)
     t_e2e = time.perf_counter() - t0
     barrier(dist, device)
     t_e2e = max_over_ranks(t_e2e, dist, device)

@@ -374,7 +374,9 @@ def run_ours(args):
     eng = P.engine
     ctor, desc, share = WORKLOADS[args.workload]
     K_steps, W_steps = args.steps, args.warmup
-    e2e_chunk = 25
+    # the host gets the traces every 100 steps: the cadence at which the reference's own loop
+    # hands its state to the host (Save_Data every 100 steps, DG_leap_Frog_OpenMP.c:433-444)
+    e2e_chunk = 100
     e2e_steps = max(e2e_chunk, (K_steps // e2e_chunk) * e2e_chunk)
     acc_steps = 1000   # FP32 against FP64: long enough for arrivals at the receivers of every workload
     table = max(W_steps + 2 * K_steps, W_steps + e2e_steps, acc_steps) + 8

@@ -339,16 +339,21 @@ def run_reference_arm(args):
     return 0
 
 
-def read_traffic(workload: str, kernel: str):
-    """DRAM bytes per launch from the committed ncu summary (profiles/), if one exists."""
-    p = os.path.join(ROOT, "profiles", "traffic_%s_%s.txt" % (kernel, workload))
-    try:
-        with open(p) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1])
-    except OSError:
-        pass
+def read_traffic(workload: str, kernel: str, precision: str = "fp32"):
+    """DRAM bytes per launch from the committed ncu summary (profiles/), if one exists: the file
+    for this arithmetic (traffic_<kernel>_<workload>_<precision>.txt), or for FP32 the one
+    without the suffix."""
+    names = ["traffic_%s_%s_%s.txt" % (kernel, workload, precision)]
+    if precision == "fp32":
+        names.append("traffic_%s_%s.txt" % (kernel, workload))
+    for name in names:
+        try:
+            with open(os.path.join(ROOT, "profiles", name)) as f:
+                for line in f:
+                    if line.startswith("traffic_bytes_per_launch:"):
+                        return float(line.split(":", 1)[1])
+        except OSError:
+            continue
     return None
 
 
@@ -428,7 +433,7 @@ def run_ours(args):
         time_source = ("a separate run of %d steps after the timed region, CUDA events around every launch"
                        % K_steps)
     achieved = dom[1] / (dom[2] * 1e-3) / 1e9
-    traffic = read_traffic(args.workload, dom[0])
+    traffic = read_traffic(args.workload, dom[0], args.precision)
     S_tot = sum(x.shots for x in ws)
     K_tot = sum(x.K for x in ws)
     R_tot = sum(x.shots * x.rec.shape[0] for x in ws)

@@ -137,6 +137,15 @@ __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
 }
 __device__ __forceinline__ int ld_volatile_i32(const int* p) { return *(volatile const int*)p; }
 
+// 8 bytes from global to this thread's shared memory without a register (cp.async, through
+// L1), the group commit, and the wait for this thread's copies
+__device__ __forceinline__ void cp_async8(void* dst_smem, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <class R> __device__ __forceinline__ R ldg(const R* p) { return __ldg(p); }
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 __device__ __forceinline__ double4 ld4(const double4* p) {

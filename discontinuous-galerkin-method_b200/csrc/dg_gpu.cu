@@ -132,6 +132,7 @@ struct dg_gpu_ctx {
   bool x2pm = false; // the two-shot bodies on the plane-major layout (MeshDev::kind 3)
   bool wave = false;  // one launch per step (k_step_wave / k_step_wave_p), RCM order, schedule in wv
   bool wave_persistent = false;  // k_step_wave_p: resident blocks looping over the tickets
+  bool wave_async = false;       // ... with the old values staged in shared memory by cp.async
   int margin_warps_per_sm = 10;  // lag margin of the wavefront step beyond the unit bandwidth
   int blocks_p = 0;              // its grid
   Wave wv{};
@@ -703,6 +704,13 @@ template <class R> int layout(dg_gpu_ctx* c, std::vector<MeshDev<R>>& md, MeshDe
 
 int wave_resident(dg_gpu_ctx* c, int& per_sm);
 
+// dynamic shared memory of a wavefront launch: the staging slots of the async layout
+size_t wave_smem(const dg_gpu_ctx* c) {
+  if (!c->wave_persistent || !c->wave_async) return 0;
+  const size_t slots = c->kahan ? wave_stage_slots<true>() : wave_stage_slots<false>();
+  return (size_t)(c->block / 32) * slots * 32 * sizeof(float2);
+}
+
 // Sets the ticket counter to the step the counters hold, for a launch grid of G blocks.
 __global__ void k_wave_sync(const Counters* __restrict__ ctr, unsigned long long* tickets, unsigned G) {
   *tickets = (unsigned long long)ctr->v * G;
@@ -893,9 +901,10 @@ int launch_x2(dg_gpu_ctx* c, cudaEvent_t mid, bool hv = true, bool ht = true) {
 // resident blocks of the persistent wavefront kernel for the current block size
 int wave_resident(dg_gpu_ctx* c, int& per_sm) {
   per_sm = 0;
-  const WaveFn k = kernel_wave(c->x2, c->kahan, true);
+  const WaveFn k = c->wave_async ? kernel_wave_async(c->x2, c->kahan) : kernel_wave(c->x2, c->kahan, true);
   if (!k) return fail(DG_ERR_UNSUPPORTED, "no wavefront step for this shot count");
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, c->block, 0);
+  if (wave_smem(c) > 48 * 1024) CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wave_smem(c)));
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, c->block, wave_smem(c));
   if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __LINE__);
   return DG_OK;
 }
@@ -904,10 +913,11 @@ int wave_resident(dg_gpu_ctx* c, int& per_sm) {
 bool wave_supported(int S) { return S == 2 || S == 4 || S == 8 || S == 16 || S == 32 || S == 64 || S == 128; }
 
 int launch_wave(dg_gpu_ctx* c) {
-  const WaveFn k = kernel_wave(c->x2, c->kahan, c->wave_persistent);
+  const bool as = c->wave_persistent && c->wave_async;
+  const WaveFn k = as ? kernel_wave_async(c->x2, c->kahan) : kernel_wave(c->x2, c->kahan, c->wave_persistent);
   if (!k) return fail(DG_ERR_UNSUPPORTED, "no wavefront step for this shot count");
   const dim3 bl(c->block), g(c->wave_persistent ? c->blocks_p : c->blocks_v);
-  k<<<g, bl, 0, c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr);
+  k<<<g, bl, wave_smem(c), c->stream>>>(c->ops2, c->md_f[0], c->wv, c->d_ctr);
   return DG_OK;
 }
 
@@ -1324,6 +1334,11 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   c->wave_persistent = c->wave && c->x2 >= 2;
   if (const char* env = getenv("DG_WAVE_PERSISTENT"))
     if (c->wave) c->wave_persistent = atoi(env) != 0;
+  // FP32 on the persistent form: the old values staged in shared memory by cp.async (200k x 64
+  // batch: 0.6166 against 0.6245 ms a step, the same bits; FP32-Kahan, which stages twice as many,
+  // 1.13 against 1.04, keeps the plain form; DG_WAVE_ASYNC=0/1 overrides)
+  c->wave_async = c->x2 >= 16 && !c->kahan;
+  if (const char* env = getenv("DG_WAVE_ASYNC")) c->wave_async = c->x2 >= 16 && atoi(env) != 0;
   if (const char* env = getenv("DG_PDL")) c->pdl = atoi(env) != 0;
   if (c->mx) {
     if ((rc = c->alloc(&c->d_mxbar, 2))) return rc;

@@ -4,6 +4,15 @@
 
 namespace dg {
 
+WaveFn kernel_wave_async(int S, bool kahan) {
+#define DG_WVA(SS, KH) \
+  if (S == SS && kahan == KH) return (WaveFn)k_step_wave_p<WaveTwoShotsAsync<SS>, KH>;
+  DG_WVA(16, false) DG_WVA(16, true) DG_WVA(32, false) DG_WVA(32, true) DG_WVA(64, false) DG_WVA(64, true)
+  DG_WVA(128, false) DG_WVA(128, true)
+#undef DG_WVA
+  return nullptr;
+}
+
 WaveFn kernel_wave(int S, bool kahan, bool persistent) {
 #define DG_WV(SS, LAYOUT, KH)                                            \
   if (S == SS && kahan == KH)                                            \

@@ -32,6 +32,9 @@ HalfPair<GenFn<float>> kernels_fp32(bool kahan, bool multi);      // dg_k_generi
 HalfPair<GenFn<double>> kernels_reference(bool multi, bool otf);  // dg_k_generic.cu
 // S shots (2..128, powers of two), or S = 1 on the one-shot layout
 WaveFn kernel_wave(int S, bool kahan, bool persistent);           // dg_k_wave.cu
+// the resident-block form whose halves stage the element's old values in shared memory
+// (S = 16 .. 128); dynamic shared memory: wave_stage_slots<kahan>() * 32 float2 per warp
+WaveFn kernel_wave_async(int S, bool kahan);                      // dg_k_wave.cu
 HalfPair<MxFn> kernels_batch(bool kahan);                         // dg_k_multi.cu
 MxpFn kernel_batch_persistent(bool kahan);                        // dg_k_multi.cu
 

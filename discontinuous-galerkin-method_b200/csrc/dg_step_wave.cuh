@@ -110,6 +110,34 @@ struct WaveTwoShots {  // element-major U[e][plane][S], thread g: element g / (S
   }
 };
 
+// The two-shot layout whose halves request the element's own old values (velocities and
+// compensations in the velocity half, stresses and compensations in the stress half) into
+// shared memory at their start (cp.async, no registers held) and read them from there for the
+// update.  Each warp has wave_stage_slots<KAHAN>() float2 per lane of the block's dynamic shared
+// memory; the two halves of a ticket reuse them one after the other.
+template <bool KAHAN> __host__ __device__ constexpr int wave_stage_slots() { return KAHAN ? 36 : 18; }
+
+template <int S>
+struct WaveTwoShotsAsync : WaveTwoShots<S> {
+  using Pre = StressConst;
+  template <bool KAHAN>
+  static __device__ __forceinline__ float2* stage() {
+    extern __shared__ float2 wave_stage[];
+    return wave_stage + (threadIdx.x >> 5) * (wave_stage_slots<KAHAN>() * 32) + (threadIdx.x & 31);
+  }
+  template <bool KAHAN>
+  static __device__ __forceinline__ void velocity(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
+    velocity_x2_body<S, KAHAN, false, true>(ops, m, lb, t, stage<KAHAN>());
+  }
+  template <bool KAHAN>
+  static __device__ __forceinline__ void stress(const Ops2& ops, const MeshDev<float>& m, int lb, long long t,
+                                                const Pre& sc) {
+    constexpr int H = S / 2;
+    const int g = lb * (int)blockDim.x + (int)threadIdx.x;
+    if (g < m.K * H) stress_x2_core<S, KAHAN, true, false, true>(ops, m, g / H, g - (g / H) * H, sc, stage<KAHAN>());
+  }
+};
+
 struct WaveOneShot {  // plane-major U[plane][Kp], thread p: elements 2p and 2p+1
   struct Pre {};
   template <bool KAHAN>

@@ -46,8 +46,12 @@ __device__ __forceinline__ void kahan2(float2& u, float2& c, float2 d) {
 // wrappers below (one mesh) and the multi-mesh dispatchers (dg_step_multi.cuh) call them.
 // PM: plane-major layout U[plane][e*S + s] (plane stride Kp*S/2 float2) instead of the
 // element-major U[e][plane][S]; the arithmetic is the same.
-template <int S, bool KAHAN, bool PM = false>
-__device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t) {
+// ASYNC (the wavefront step): the element's own velocities (and compensations) are requested at
+// the start into this thread's slots of `stage` (stage[plane * 32], cp.async: no registers held)
+// and read from there for the update, so their round trip overlaps the stress loads'.
+template <int S, bool KAHAN, bool PM = false, bool ASYNC = false>
+__device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<float>& m, int lb, long long t,
+                                                 float2* stage = nullptr) {
   constexpr int H = S / 2;    // float2 lanes per element
   constexpr int ES = 30 * H;  // element stride in float2 (element-major)
   const long long EO = PM ? H : ES;                   // element offset
@@ -56,6 +60,16 @@ __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<
   if (g >= m.K * H) return;
   const int e = g / H, q = g - e * H;
   float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * EO + q;
+  if constexpr (ASYNC) {
+#pragma unroll
+    for (int i = 0; i < 12; i++) cp_async8(stage + i * 32, Ue + i * PS);
+    if (KAHAN) {
+      const float2* Ce0 = reinterpret_cast<const float2*>(m.C) + (long long)e * EO + q;
+#pragma unroll
+      for (int i = 0; i < 12; i++) cp_async8(stage + (12 + i) * 32, Ce0 + i * PS);
+    }
+    cp_async_commit();
+  }
 
   float2 txx[NP], tzz[NP], txz[NP];
 #pragma unroll
@@ -156,13 +170,23 @@ __device__ __forceinline__ void velocity_x2_body(const Ops2& ops, const MeshDev<
 
   // V = a V (+ source on Vz) + dt/rho * rhs
   float2 vx[NP], vz[NP], cx[NP], cz[NP];
-#pragma unroll
-  for (int i = 0; i < NP; i++) { vx[i] = Ue[(0 + i) * PS]; vz[i] = Ue[(6 + i) * PS]; }
   float2* __restrict__ Ce = nullptr;
-  if (KAHAN) {
-    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * EO + q;
+  if (KAHAN) Ce = reinterpret_cast<float2*>(m.C) + (long long)e * EO + q;
+  if constexpr (ASYNC) {
+    cp_async_wait_all();
 #pragma unroll
-    for (int i = 0; i < NP; i++) { cx[i] = Ce[(0 + i) * PS]; cz[i] = Ce[(6 + i) * PS]; }
+    for (int i = 0; i < NP; i++) { vx[i] = stage[(0 + i) * 32]; vz[i] = stage[(6 + i) * 32]; }
+    if (KAHAN) {
+#pragma unroll
+      for (int i = 0; i < NP; i++) { cx[i] = stage[(12 + i) * 32]; cz[i] = stage[(18 + i) * 32]; }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < NP; i++) { vx[i] = Ue[(0 + i) * PS]; vz[i] = Ue[(6 + i) * PS]; }
+    if (KAHAN) {
+#pragma unroll
+      for (int i = 0; i < NP; i++) { cx[i] = Ce[(0 + i) * PS]; cz[i] = Ce[(6 + i) * PS]; }
+    }
   }
   if (own_sponge) {
 #pragma unroll
@@ -232,14 +256,26 @@ __device__ __forceinline__ StressConst stress_const(const MeshDev<float>& m, int
 }
 
 // Stress update of lane q (shots 2q, 2q+1) of element e with its constants already loaded.
-template <int S, bool KAHAN, bool FRESH, bool PM = false>
+// ASYNC: the element's own stresses (and compensations) are requested at the start into this
+// thread's slots of `stage` and read from there for the update (see velocity_x2_body).
+template <int S, bool KAHAN, bool FRESH, bool PM = false, bool ASYNC = false>
 __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<float>& m, int e, int q,
-                                               const StressConst& k) {
+                                               const StressConst& k, float2* stage = nullptr) {
   constexpr int H = S / 2;
   constexpr int ES = 30 * H;
   const long long EO = PM ? H : ES;                   // element offset
   const long long PS = PM ? (long long)m.Kp * H : H;  // plane stride
   float2* __restrict__ Ue = reinterpret_cast<float2*>(m.U) + (long long)e * EO + q;
+  if constexpr (ASYNC) {
+#pragma unroll
+    for (int i = 0; i < 18; i++) cp_async8(stage + i * 32, Ue + (12 + i) * PS);
+    if (KAHAN) {
+      const float2* Ce0 = reinterpret_cast<const float2*>(m.C) + (long long)e * EO + q;
+#pragma unroll
+      for (int i = 0; i < 18; i++) cp_async8(stage + (18 + i) * 32, Ce0 + (12 + i) * PS);
+    }
+    cp_async_commit();
+  }
 
   float2 vx[NP], vz[NP];
 #pragma unroll
@@ -311,17 +347,33 @@ __device__ __forceinline__ void stress_x2_core(const Ops2& ops, const MeshDev<fl
   }
 
   float2 txx[NP], tzz[NP], txz[NP], cxx[NP], czz[NP], cxz[NP];
-#pragma unroll
-  for (int i = 0; i < NP; i++) {
-    txx[i] = Ue[(12 + i) * PS];
-    tzz[i] = Ue[(18 + i) * PS];
-    txz[i] = Ue[(24 + i) * PS];
-  }
   float2* __restrict__ Ce = nullptr;
-  if (KAHAN) {
-    Ce = reinterpret_cast<float2*>(m.C) + (long long)e * EO + q;
+  if (KAHAN) Ce = reinterpret_cast<float2*>(m.C) + (long long)e * EO + q;
+  if constexpr (ASYNC) {
+    cp_async_wait_all();
 #pragma unroll
-    for (int i = 0; i < NP; i++) { cxx[i] = Ce[(12 + i) * PS]; czz[i] = Ce[(18 + i) * PS]; cxz[i] = Ce[(24 + i) * PS]; }
+    for (int i = 0; i < NP; i++) {
+      txx[i] = stage[(0 + i) * 32];
+      tzz[i] = stage[(6 + i) * 32];
+      txz[i] = stage[(12 + i) * 32];
+    }
+    if (KAHAN) {
+#pragma unroll
+      for (int i = 0; i < NP; i++) {
+        cxx[i] = stage[(18 + i) * 32]; czz[i] = stage[(24 + i) * 32]; cxz[i] = stage[(30 + i) * 32];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < NP; i++) {
+      txx[i] = Ue[(12 + i) * PS];
+      tzz[i] = Ue[(18 + i) * PS];
+      txz[i] = Ue[(24 + i) * PS];
+    }
+    if (KAHAN) {
+#pragma unroll
+      for (int i = 0; i < NP; i++) { cxx[i] = Ce[(12 + i) * PS]; czz[i] = Ce[(18 + i) * PS]; cxz[i] = Ce[(24 + i) * PS]; }
+    }
   }
   if (fc.w & 1) {
 #pragma unroll

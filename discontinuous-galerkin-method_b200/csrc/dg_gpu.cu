@@ -176,6 +176,17 @@ struct dg_gpu_ctx {
   double* snap_dev = nullptr;
   double* snap_host = nullptr;
   size_t snap_elems = 0;  // doubles per field and slot
+  // step marks: an event recorded on the context stream after each dg_gpu_step(_async) call and
+  // the step count it ends at, so a trace fetch on the copy stream waits for the steps that
+  // wrote its window and no later ones
+  struct StepMark {
+    long t_end = -1;
+    cudaEvent_t ev = nullptr;
+  };
+  static constexpr int kMarks = 4;
+  StepMark marks[kMarks];
+  int mark_next = 0;
+  cudaEvent_t ev_fetch = nullptr, ev_wavelet = nullptr;
 
   ~dg_gpu_ctx() {
     if (graph) cudaGraphExecDestroy(graph);
@@ -186,6 +197,10 @@ struct dg_gpu_ctx {
       if (snap_conv[k]) cudaEventDestroy(snap_conv[k]);
       if (snap_copy[k]) cudaEventDestroy(snap_copy[k]);
     }
+    for (auto& m : marks)
+      if (m.ev) cudaEventDestroy(m.ev);
+    if (ev_fetch) cudaEventDestroy(ev_fetch);
+    if (ev_wavelet) cudaEventDestroy(ev_wavelet);
     if (snap_host) cudaFreeHost(snap_host);
     if (copy_stream) cudaStreamDestroy(copy_stream);
     for (void* p : allocs) cudaFree(p);
@@ -1086,6 +1101,7 @@ int zero_state(dg_gpu_ctx* c) {
   }
   CK(cudaStreamSynchronize(c->stream));
   c->t = 0;
+  for (auto& m : c->marks) m.t_end = -1;  // no step mark covers the new run's steps
   return DG_OK;
 }
 
@@ -1231,11 +1247,17 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
   c->watchdog_every = std::max(0, o.watchdog_every);
   c->mx = c->multi && !c->is_double;
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  // the copy stream (trace fetches, wavelet uploads and snapshots beside the steps) and the
+  // step marks exist from the start, so the first fetch pays for neither
+  CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  for (auto& m : c->marks) CK(cudaEventCreateWithFlags(&m.ev, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&c->ev_fetch, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&c->ev_wavelet, cudaEventDisableTiming));
   for (auto& e : c->ev) CK(cudaEventCreate(&e));
 
   c->mi.resize(n_meshes);
   double bytes = 0, dof = 0;
-  size_t stage = 1;
+  size_t stage = 1, trace_chunk = 0;
   const size_t w = c->is_double ? 8 : 4;
   // the packed FP32 kernels carry the P2 operators as compile-time constants: other operators
   // run on the one-(element, shot)-per-thread kernels
@@ -1308,7 +1330,11 @@ int dg_gpu_init(dg_gpu_ctx** out, const dg_gpu_mesh* meshes, int n_meshes, const
     c->bytes_wave += per_wave * (double)h.K;
     dof += 30.0 * (double)h.K * h.S;
     stage = std::max(stage, (size_t)std::max<long>(h.K * 6, h.steps * std::max(1, h.n_rec)));
+    trace_chunk += (size_t)std::min<long>(100, h.steps) * h.n_rec * h.S;
   }
+  // the staging buffer also holds both components of every mesh's traces over 100 steps (one
+  // all-mesh fetch per default graph), so fetches of that size need no new allocation
+  stage = std::max(stage, 2 * trace_chunk);
   c->bytes_two_pass = bytes;
   c->stats.dof_per_step = dof;
   if (c->is_double) fill_ops(c->ops_d, meshes[0]); else fill_ops(c->ops_f, meshes[0]);
@@ -1428,6 +1454,44 @@ static int enqueue_steps(dg_gpu_ctx* c, long n, bool timed) {
   return DG_OK;
 }
 
+static int ensure_copy_stream(dg_gpu_ctx* c) {
+  if (!c->copy_stream) CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  return DG_OK;
+}
+
+static int ensure_event(cudaEvent_t* ev) {
+  if (!*ev) CK(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  return DG_OK;
+}
+
+// Records a step mark after the work enqueued so far.
+static int mark_steps(dg_gpu_ctx* c) {
+  auto& m = c->marks[c->mark_next];
+  int rc = ensure_event(&m.ev);
+  if (rc) return rc;
+  CK(cudaEventRecord(m.ev, c->stream));
+  m.t_end = c->t;
+  c->mark_next = (c->mark_next + 1) % dg_gpu_ctx::kMarks;
+  return DG_OK;
+}
+
+// The event after which steps [0, t) are complete: the earliest mark at or past t, else a new
+// event after all the work enqueued so far.
+static int steps_done_event(dg_gpu_ctx* c, long t, cudaEvent_t* out) {
+  const dg_gpu_ctx::StepMark* best = nullptr;
+  for (const auto& m : c->marks)
+    if (m.ev && m.t_end >= t && m.t_end <= c->t && (!best || m.t_end < best->t_end)) best = &m;
+  if (best) {
+    *out = best->ev;
+    return DG_OK;
+  }
+  int rc = ensure_event(&c->ev_fetch);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev_fetch, c->stream));
+  *out = c->ev_fetch;
+  return DG_OK;
+}
+
 static int do_steps(dg_gpu_ctx* c, long n, bool timed, bool wait = true) {
   if (!c || n < 0) return fail(DG_ERR_ARG, "bad arguments");
   if (c->half_pending || c->part_done)
@@ -1436,6 +1500,7 @@ static int do_steps(dg_gpu_ctx* c, long n, bool timed, bool wait = true) {
   CK(cudaSetDevice(c->device));
   int rc = enqueue_steps(c, n, timed);
   if (rc) return rc;
+  if ((rc = mark_steps(c))) return rc;
   c->stats.steps_done = c->t;
   if (!wait) return DG_OK;
   CK(cudaStreamSynchronize(c->stream));
@@ -1530,6 +1595,12 @@ int dg_gpu_fetch_traces(dg_gpu_ctx* c, int mesh, long t0, long n, double* dst_x,
   CK(cudaSetDevice(c->device));
   int rc = ensure_stage(c, (size_t)2 * total);
   if (rc) return rc;
+  // the gather and the copies run on the copy stream after the steps that wrote the window
+  // (each step's traces have their own slots), so steps enqueued after those keep running
+  cudaEvent_t written = nullptr;
+  if ((rc = ensure_copy_stream(c)) || (rc = steps_done_event(c, t0 + n, &written))) return rc;
+  cudaStream_t cs = c->copy_stream;
+  CK(cudaStreamWaitEvent(cs, written, 0));
   const int B = 256;
   long long at = 0;
   for (int k = k0; k < k1; k++) {
@@ -1540,15 +1611,15 @@ int dg_gpu_fetch_traces(dg_gpu_ctx* c, int mesh, long t0, long n, double* dst_x,
     double* ox = c->d_stage + at;
     double* oz = c->d_stage + total + at;
     if (c->is_double)
-      k_fetch_traces<double><<<grid, B, 0, c->stream>>>(c->md_d[k].trace, h.n_rec, h.S_pad, h.S, t0, n, ox, oz);
+      k_fetch_traces<double><<<grid, B, 0, cs>>>(c->md_d[k].trace, h.n_rec, h.S_pad, h.S, t0, n, ox, oz);
     else
-      k_fetch_traces<float><<<grid, B, 0, c->stream>>>(c->md_f[k].trace, h.n_rec, h.S_pad, h.S, t0, n, ox, oz);
+      k_fetch_traces<float><<<grid, B, 0, cs>>>(c->md_f[k].trace, h.n_rec, h.S_pad, h.S, t0, n, ox, oz);
     CK(cudaGetLastError());
     at += per;
   }
-  CK(cudaMemcpyAsync(dst_x, c->d_stage, total * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(dst_z, c->d_stage + total, total * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpyAsync(dst_x, c->d_stage, total * sizeof(double), cudaMemcpyDeviceToHost, cs));
+  CK(cudaMemcpyAsync(dst_z, c->d_stage + total, total * sizeof(double), cudaMemcpyDeviceToHost, cs));
+  CK(cudaStreamSynchronize(cs));
   return DG_OK;
 }
 
@@ -1590,8 +1661,8 @@ int dg_gpu_step_snapshots(dg_gpu_ctx* c, long n, long every, int mesh, int shot,
     c->snap_host = (double*)hp;
     c->snap_elems = per;
   }
-  if (!c->copy_stream) {
-    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  if (int rc = ensure_copy_stream(c)) return rc;
+  if (!c->snap_conv[0]) {
     for (int k = 0; k < 2; k++) {
       CK(cudaEventCreateWithFlags(&c->snap_conv[k], cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&c->snap_copy[k], cudaEventDisableTiming));
@@ -1922,12 +1993,22 @@ int dg_gpu_set_wavelet(dg_gpu_ctx* c, int mesh, long t0, long n, const double* w
   for (int k = k0; k < k1; k++)
     if (t0 + n > c->mi[k].steps) return fail(DG_ERR_ARG, "wavelet window beyond a mesh's steps");
   CK(cudaSetDevice(c->device));
+  // samples that no enqueued step reads (t0 at or past the steps enqueued so far) go over the
+  // copy stream, and the context stream waits for them, so steps in flight keep running;
+  // otherwise the copy follows the enqueued steps on the context stream
+  const bool ahead = t0 >= c->t;
+  int rc;
+  if (ahead && ((rc = ensure_copy_stream(c)) || (rc = ensure_event(&c->ev_wavelet)))) return rc;
+  cudaStream_t st = ahead ? c->copy_stream : c->stream;
   for (int k = k0; k < k1; k++) {  // mesh k's samples follow those of the meshes before it
     const double* dw = c->is_double ? c->md_d[k].wavelet : c->md_f[k].wavelet;
-    CK(cudaMemcpyAsync((void*)(dw + t0), w + (size_t)(k - k0) * n, n * sizeof(double), cudaMemcpyHostToDevice,
-                       c->stream));
+    CK(cudaMemcpyAsync((void*)(dw + t0), w + (size_t)(k - k0) * n, n * sizeof(double), cudaMemcpyHostToDevice, st));
   }
-  CK(cudaStreamSynchronize(c->stream));
+  if (ahead) {
+    CK(cudaEventRecord(c->ev_wavelet, st));
+    CK(cudaStreamWaitEvent(c->stream, c->ev_wavelet, 0));
+  }
+  CK(cudaStreamSynchronize(st));
   return DG_OK;
 }
 

@@ -138,7 +138,9 @@ int dg_gpu_step(dg_gpu_ctx *ctx, long n);
 /* The same steps, enqueued on the context stream without waiting for them (with the NaN
  * watchdog on, its checks still wait): the host is free until dg_gpu_synchronize, which waits
  * and reports a wait limit reached on the way (DG_ERR_TIMEOUT).  Every other call of the context
- * is ordered after the enqueued steps (fetches wait for them). */
+ * is ordered after the enqueued steps (fetches wait for them), except dg_gpu_fetch_traces of
+ * steps an earlier step call completes and dg_gpu_set_wavelet of samples no enqueued step reads,
+ * which run on a second stream while the later steps keep running. */
 int dg_gpu_step_async(dg_gpu_ctx *ctx, long n);
 int dg_gpu_synchronize(dg_gpu_ctx *ctx);
 
@@ -157,7 +159,10 @@ int dg_gpu_step_profiled(dg_gpu_ctx *ctx, long n, int flush_l2, float *ms_vel, f
 /* Receiver traces of steps [t0, t0+n) for every shot of one mesh:
  * dst_x / dst_z = double[n_shots][n][n_rec] (each shot like the reference's record_x window).
  * mesh = DG_ALL_MESHES: those blocks of every mesh one after the other, in mesh order, with one
- * synchronisation. */
+ * synchronisation.  The call waits for the steps that wrote the window and returns with the
+ * copies done; when a dg_gpu_step / dg_gpu_step_async call ended at or past step t0+n, it waits
+ * for that call's steps only, so steps enqueued after it keep running meanwhile (a fetch of
+ * chunk c overlaps the steps of chunk c+1). */
 #define DG_ALL_MESHES (-1)
 int dg_gpu_fetch_traces(dg_gpu_ctx *ctx, int mesh, long t0, long n, double *dst_x, double *dst_z);
 
@@ -176,7 +181,9 @@ int dg_gpu_reset(dg_gpu_ctx *ctx);
 
 /* Replace wavelet samples [t0, t0+n) of one mesh with host values (the reference computes
  * w(t) on the host every step, DG_leap_Frog_OpenMP.c:421); mesh = DG_ALL_MESHES: w holds n
- * samples for each mesh, one after the other in mesh order. */
+ * samples for each mesh, one after the other in mesh order.  Returns with w copied.  Steps
+ * enqueued before the call that read these samples see the old ones; when none does (t0 at or
+ * past the steps enqueued so far) the copy does not wait for the steps in flight. */
 int dg_gpu_set_wavelet(dg_gpu_ctx *ctx, int mesh, long t0, long n, const double *w);
 
 /* ---- one mesh split over several contexts (one per GPU): domain decomposition --------------

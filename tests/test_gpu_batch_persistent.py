@@ -139,6 +139,62 @@ def test_async_steps_equal_synchronous_steps(meshes, precision, wave):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision,wave", [("fp32", -1), ("fp32", 0), ("fp64", -1)])
+def test_overlapped_chunks_equal_synchronous_chunks(meshes, precision, wave):
+    """The end-to-end loop with overlap: the next chunk's wavelet uploaded while the current chunk
+    steps (samples no enqueued step reads), its steps enqueued, then the previous chunk's traces
+    fetched while they run, gives the traces and fields of the synchronous loop bit for bit."""
+    chunk, n_chunks = 30, 5
+    rng = np.random.default_rng(7)
+    wav = rng.standard_normal(chunk * n_chunks) * 1e-2
+    out = []
+    for overlap in (False, True):
+        with eng.Engine(meshes[3], precision, wavefront=wave) as e:   # 16 shots
+            got = [None] * n_chunks
+            for c in range(n_chunks):
+                e.set_wavelet(c * chunk, wav[c * chunk:(c + 1) * chunk])
+                if overlap:
+                    e.step_async(chunk)
+                    if c > 0:
+                        got[c - 1] = e.fetch_traces((c - 1) * chunk, chunk)
+                else:
+                    e.step(chunk)
+                    got[c] = e.fetch_traces(c * chunk, chunk)
+            if overlap:
+                got[-1] = e.fetch_traces((n_chunks - 1) * chunk, chunk)
+                e.synchronize()
+            out.append([np.concatenate([g[i] for g in got], axis=1) for i in (0, 1)] +
+                       [e.fetch("Vz", 0, s) for s in (0, 15)])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+    assert np.abs(out[0][1]).max() > 0
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_wavelet_update_after_enqueued_steps(meshes, precision):
+    """Samples that enqueued steps read are replaced only after those steps (the copy follows
+    them); a fetch of a window that no single step call ends at waits for all enqueued work."""
+    new = np.full(40, 5e-3)
+    out = []
+    for use_async in (False, True):
+        with eng.Engine(meshes[3], precision) as e:
+            if use_async:
+                e.step_async(25)
+                e.step_async(15)
+                e.set_wavelet(20, new)         # steps 20..39 are in flight: they keep the old samples
+                e.step_async(40)
+                tr = e.fetch_traces(10, 50)   # ends inside the second 40-step call
+                e.synchronize()
+            else:
+                e.step(40)
+                e.set_wavelet(20, new)
+                e.step(40)
+                tr = e.fetch_traces(10, 50)
+            out.append(list(tr) + [e.fetch("Vz", 0, 3)])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 def test_fetch_every_shot_at_once(meshes, precision):
     """DG_ALL_SHOTS: one call returns a field of every shot of a mesh, equal to the per-shot calls."""

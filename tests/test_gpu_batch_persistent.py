@@ -170,6 +170,36 @@ def test_overlapped_chunks_equal_synchronous_chunks(meshes, precision, wave):
     assert np.abs(out[0][1]).max() > 0
 
 
+@pytest.mark.parametrize("persistent", [True, False])
+def test_overlapped_chunks_every_mesh(meshes, monkeypatch, persistent):
+    """The same overlapped loop over the whole batch (one wavelet upload and one trace fetch for
+    every mesh, DG_ALL_MESHES), in the persistent cooperative launch and in two launches a step:
+    a fetch's gather on the copy stream runs beside the next chunk's grid."""
+    monkeypatch.setenv("DG_MX_PERSISTENT", "1" if persistent else "0")
+    chunk, n_chunks = 30, 3
+    rng = np.random.default_rng(11)
+    wav = rng.standard_normal((len(SPEC), chunk * n_chunks)) * 1e-2
+    out = []
+    for overlap in (False, True):
+        with eng.Engine(meshes, "fp32") as e:
+            got = [None] * n_chunks
+            for c in range(n_chunks):
+                e.set_wavelet(c * chunk, wav[:, c * chunk:(c + 1) * chunk].ravel(), mesh=eng.ALL_MESHES)
+                if overlap:
+                    e.step_async(chunk)
+                    if c > 0:
+                        got[c - 1] = e.fetch_traces((c - 1) * chunk, chunk, mesh=eng.ALL_MESHES)
+                else:
+                    e.step(chunk)
+                    got[c] = e.fetch_traces(c * chunk, chunk, mesh=eng.ALL_MESHES)
+            if overlap:
+                got[-1] = e.fetch_traces((n_chunks - 1) * chunk, chunk, mesh=eng.ALL_MESHES)
+                e.synchronize()
+            out.append([g[i] for g in got for i in (0, 1)] + [e.fetch("Vz", k, 0) for k in range(len(SPEC))])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 def test_wavelet_update_after_enqueued_steps(meshes, precision):
     """Samples that enqueued steps read are replaced only after those steps (the copy follows
